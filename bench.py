@@ -1,0 +1,339 @@
+#!/usr/bin/env python
+"""J/K build throughput on one B200 (or N independent replicas).
+
+A step is one direct-SCF J/K build (FP64 J and K of one density) of the
+workload, through the engine's entry jk_get_jk with the density resident on
+the device (``value``), and end to end through the public get_jk call with
+host numpy input and output (``e2e``).  Default workload: a seeded (H2O)32
+cluster in a 14 A cube with the def2-TZVP stand-in basis (s-f shells, 1376
+spherical functions), density D = 2 C C^T with C^T S C = 1.
+
+Timing: CUDA events on the launching stream around each step, L2 flushed
+(a 512 MiB buffer written) before every timed step, max over ranks.
+The CPU baseline is the oracle (the OpenMP restatement of the reference's
+algorithm) on the host cores, timed on a uniform subsample of shell-pair rows
+and scaled to a full build.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (nwater, cube A, seed, basis)
+    'h2o32-tzvp': (32, 14.0, 2, 'standin-def2-tzvp'),
+    'h2o8-dz': (8, 9.0, 0, 'standin-cc-pvdz'),
+    'h2o64-dz': (64, 18.0, 3, 'standin-cc-pvdz'),
+}
+
+
+def make_workload(name):
+    from byteqc_b200.gto import Mole, geom
+    nw, box, seed, basis = WORKLOADS[name]
+    mol = Mole(atom=geom.water_cluster(nw, box=box, seed=seed),
+               basis=basis).build()
+    s = mol.intor('int1e_ovlp')
+    dm = geom.scf_like_density(s, nocc=mol.nelectron // 2, seed=1)
+    return mol, dm
+
+
+def ncart(l):
+    return (l + 1) * (l + 2) // 2
+
+
+def class_flops(li, lj, lk, ll, nprim_ij, nprim_kl, n_dm=1, with_j=True,
+                with_k=True):
+    """Algorithmic FLOPs of one contracted quartet of the class: the fixed
+    cost model used for the roofline (identical for every engine)."""
+    n = (li + lj + lk + ll) // 2 + 1
+    nm, mm = li + lj, lk + ll
+    nf = ncart(li) * ncart(lj) * ncart(lk) * ncart(ll)
+    vrr = 4 * nm + 6 * (nm + 1) * mm
+    hrr = 2 * sum((nm - j + 1) * (mm + 1) for j in range(1, lj + 1))
+    hrr += 2 * (li + 1) * (lj + 1) * sum(mm - l + 1 for l in range(1, ll + 1))
+    per_root = 56 + 20 + 3 * (vrr + hrr) + 3 * nf
+    prim = 30 + n * per_root
+    dig = (4 * nf if with_j else 0) + (8 * nf if with_k else 0)
+    return nprim_ij * nprim_kl * prim + dig * n_dm
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clocks and throttle reasons while running."""
+
+    FIELDS = ('clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+              'clocks_event_reasons.hw_slowdown,'
+              'clocks_event_reasons.hw_thermal_slowdown,'
+              'clocks_event_reasons.sw_thermal_slowdown,'
+              'clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._th = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(
+                    ['nvidia-smi', '-i', str(self.index),
+                     '--query-gpu=' + self.FIELDS,
+                     '--format=csv,noheader,nounits'],
+                    capture_output=True, text=True, timeout=5).stdout
+                self.samples.append([v.strip() for v in out.split(',')])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._th = threading.Thread(target=self._run, daemon=True)
+        self._th.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._th.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': [],
+                    'samples': 0}
+        sm = [float(s[0]) for s in self.samples if s[0].replace('.', '').isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace('.', '').isdigit()]
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown',
+                 'sw_power_cap']
+        reasons = set()
+        for s in self.samples:
+            for n, v in zip(names, s[4:8]):
+                if v.strip().lower() == 'active':
+                    reasons.add(n)
+        return {'sm_mhz': float(np.median(sm)) if sm else None,
+                'sm_max_mhz': max(mx) if mx else None,
+                'reasons': sorted(reasons), 'samples': len(self.samples)}
+
+
+def cpu_baseline(mol, dm, target_s=15.0):
+    """Oracle J/K on all host cores over a uniform subsample of ij rows,
+    scaled to one full build.  Returns (builds/s, info)."""
+    from oracle import hf_oracle
+    opt = hf_oracle.VHFOpt(mol).build()
+    t = time.perf_counter()
+    hf_oracle.get_jk(mol, dm, vhfopt=opt, ij_stride=4096)
+    t0 = time.perf_counter() - t
+    full = t0 * 4096
+    stride = 1
+    while full / stride > target_s and stride < 4096:
+        stride *= 2
+    st = {}
+    t = time.perf_counter()
+    hf_oracle.get_jk(mol, dm, vhfopt=opt, ij_stride=stride, stats=st)
+    dt = time.perf_counter() - t
+    est = dt * stride
+    cores = int(os.environ.get('OMP_NUM_THREADS', os.cpu_count() or 1))
+    return 1.0 / est, {'cores': cores, 'stride': stride, 'sample_s': dt,
+                       'sample_quartets': st.get('quartets')}
+
+
+def run_reference(args):
+    rank = int(os.environ.get('RANK', '0'))
+    if rank != 0:
+        return
+    mol, dm = make_workload(args.workload)
+    vals = []
+    info = None
+    for i in range(args.warmup + args.steps):
+        v, info = cpu_baseline(mol, dm, target_s=args.ref_sample_s)
+        if i >= args.warmup:
+            vals.append(v)
+    value = float(np.median(vals))
+    line = {
+        'impl': 'reference', 'metric': 'jk_builds_per_s', 'value': value,
+        'unit': 'builds/s', 'n_gpus': args.gpus, 'steps': args.steps,
+        'warmup': args.warmup, 'higher_is_better': True, 'dtype': 'f64',
+        'data': 'synthetic', 'scaling': 'weak',
+        'config': {'workload': args.workload},
+        'cpu_baseline': {
+            'value': value, 'unit': 'builds/s', 'cores': info['cores'],
+            'kind': 'port',
+            'sample': 'oracle J/K on every %d-th shell-pair row of each '
+                      'class pair (%.1f s of CPU work), scaled to one build'
+                      % (info['stride'], info['sample_s'])},
+        'e2e': {'value': value, 'unit': 'builds/s', 'h2d_bytes_per_step': 0,
+                'd2h_bytes_per_step': 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=5)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--workload', default='h2o32-tzvp', choices=sorted(WORKLOADS))
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--ref-sample-s', type=float, default=12.0)
+    args = ap.parse_args()
+    if args.impl == 'reference':
+        return run_reference(args)
+
+    import torch
+    from byteqc_b200.cuobc import lib as jklib
+    from byteqc_b200.cuobc.scf import hf
+
+    rank = int(os.environ.get('RANK', '0'))
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=300))
+
+    lib = jklib.load_library()
+    mol, dm = make_workload(args.workload)
+    t = time.perf_counter()
+    opt = hf._VHFOpt(mol).build()
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t
+    nao, nao0 = opt.coeff.shape
+    stream = torch.cuda.current_stream()
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    d_dm = torch.as_tensor(dm, device='cuda').reshape(1, nao0, nao0).contiguous()
+    d_vj = torch.empty_like(d_dm)
+    d_vk = torch.empty_like(d_dm)
+    opts = jklib.JKOpts()
+    opts.direct_scf_tol = opt.direct_scf_tol
+    opts.nbins = opt.default_nbins()
+    opts.prescreen = 1
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float64, device='cuda')
+
+    def step_device():
+        jklib.check(lib.jk_get_jk(opt.handle, opt.coeff_dev.data_ptr(), nao0,
+                                  d_dm.data_ptr(), 1, d_vj.data_ptr(),
+                                  d_vk.data_ptr(), ctypes.byref(opts), sptr),
+                    'jk_get_jk')
+
+    # working-basis density for the kernel-only timing
+    C = opt.coeff_dev
+    d_w = (C @ d_dm[0] @ C.T).contiguous()
+    w_vj = torch.zeros(nao, nao, dtype=torch.float64, device='cuda')
+    w_vk = torch.zeros_like(w_vj)
+
+    def step_kernels():
+        jklib.check(lib.jk_build(opt.handle, d_w.data_ptr(), 1,
+                                 w_vj.data_ptr(), w_vk.data_ptr(),
+                                 ctypes.byref(opts), sptr), 'jk_build')
+
+    def timed(fn, n):
+        tot = 0.
+        for _ in range(n):
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            tot += e0.elapsed_time(e1)
+        return tot / n
+
+    for _ in range(args.warmup):
+        step_device()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ms_step = timed(step_device, args.steps)
+        ms_kern = timed(step_kernels, args.steps)
+    torch.cuda.synchronize()
+    # end-to-end through the public call: host numpy in, host numpy out
+    for _ in range(1):
+        hf.get_jk(mol, dm, vhfopt=opt)
+
+    def step_e2e():
+        hf.get_jk(mol, dm, vhfopt=opt)
+    ms_e2e = timed(step_e2e, max(2, args.steps // 2))
+    if dist:
+        t = torch.tensor([ms_step, ms_kern, ms_e2e], device='cuda')
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step, ms_kern, ms_e2e = t.tolist()
+
+    # quartet counts and the FLOP model
+    info = np.zeros(7, dtype=np.int32)
+    lib.jk_basis_info(opt.handle, info.ctypes.data)
+    ncq = int(info[6])
+    cq = np.zeros((max(ncq, 1), 8), dtype=np.int32)
+    lib.jk_basis_cq_info(opt.handle, cq.ctypes.data)
+    counts = np.zeros(max(ncq, 1), dtype=np.int64)
+    lib.jk_last_counts(opt.handle, counts.ctypes.data, sptr)
+    quartets = int(counts[:ncq].sum())
+    flops = sum(int(c) * class_flops(*cq[i, 2:8]) for i, c in
+                enumerate(counts[:ncq]) if c)
+    peak = ctypes.c_double()
+    lib.jk_fma_peak(0, ctypes.byref(peak))
+    achieved = flops / (ms_kern * 1e-3) / 1e12
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    line = {
+        'metric': 'jk_builds_per_s',
+        'value': world * 1e3 / ms_step,
+        'unit': 'builds/s',
+        'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
+        'ms_per_step': ms_step, 'higher_is_better': True, 'scaling': 'weak',
+        'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+        'config': {'workload': args.workload,
+                   'molecule': '(H2O)%d' % WORKLOADS[args.workload][0],
+                   'basis': WORKLOADS[args.workload][3],
+                   'nao': int(nao0), 'nao_working': int(nao),
+                   'parallelism': 'replicas' if world > 1 else 'single',
+                   'l2': 'flushed (512 MiB write) before every timed step',
+                   'direct_scf_tol': opt.direct_scf_tol,
+                   'nbins': int(opts.nbins)},
+        'quartets_per_build': quartets,
+        'quartets_per_s': world * quartets / (ms_step * 1e-3),
+        'kernel_ms_per_build': ms_kern,
+        'setup_s': setup_s,
+        'gpu_launches': 2 + int((counts[:ncq] >= 0).sum()) + 2,
+        'roofline': {'bound': 'fp64', 'achieved': achieved,
+                     'peak': peak.value, 'unit': 'TFLOP/s',
+                     'frac': achieved / peak.value if peak.value else None,
+                     'peak_source': 'measured FP64 FMA-chain kernel '
+                                    '(jk_fma_peak) in this process',
+                     'flops_per_build': flops, 'traffic': None},
+        'e2e': {'value': world * 1e3 / ms_e2e, 'unit': 'builds/s',
+                'h2d_bytes_per_step': int(dm.nbytes),
+                'd2h_bytes_per_step': int(2 * dm.nbytes)},
+        'clocks': clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        v, inf = cpu_baseline(mol, dm)
+        line['cpu_baseline'] = {
+            'value': v, 'unit': 'builds/s', 'cores': inf['cores'],
+            'kind': 'port',
+            'sample': 'oracle J/K on every %d-th shell-pair row of each class '
+                      'pair (%.1f s of CPU work), scaled to one build'
+                      % (inf['stride'], inf['sample_s'])}
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

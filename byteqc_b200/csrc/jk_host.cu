@@ -1,0 +1,859 @@
+// C-ABI of the J/K engine (declared in include/byteqc_jk.h): basis setup with
+// device-side Schwarz screening, the per-call density screen and quartet
+// enumeration on the device, the class launches, and the AO transforms.
+#include <cublas_v2.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/byteqc_jk.h"
+#include "jk_launch.cuh"
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+
+static int set_err(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CUDA_TRY(x)                                                                               \
+    do {                                                                                          \
+        cudaError_t e_ = (x);                                                                     \
+        if (e_ != cudaSuccess) return set_err(JK_ERR_CUDA, "%s: %s", #x, cudaGetErrorString(e_)); \
+    } while (0)
+
+extern "C" const char* jk_last_error(void) { return g_err.c_str(); }
+
+// ---------------------------------------------------------------------------
+// launcher tables
+// ---------------------------------------------------------------------------
+static jk_launch_fn g_tab64[256], g_tab32[256];
+static std::once_flag g_tab_once;
+static void init_tables() {
+    std::call_once(g_tab_once, [] {
+        jk_register_l0(g_tab64, g_tab32);
+        jk_register_l1(g_tab64, g_tab32);
+        jk_register_l2(g_tab64, g_tab32);
+        jk_register_l3a(g_tab64, g_tab32);
+        jk_register_l3b(g_tab64, g_tab32);
+    });
+}
+
+// libcint slots (cuobc/lib/gint/gint.h:29-46)
+#define ATM_SLOTS 6
+#define PTR_COORD 1
+#define BAS_SLOTS 8
+#define ATOM_OF 0
+#define ANG_OF 1
+#define NPRIM_OF 2
+#define NCTR_OF 3
+#define PTR_EXP 5
+#define PTR_COEFF 6
+
+static double common_fac_sp(int l) {
+    return l == 0 ? 0.282094791773878143 : (l == 1 ? 0.488602511902919921 : 1.0);
+}
+
+// ---------------------------------------------------------------------------
+// Schwarz matrix on the device: q[i,j] = sqrt(max_{a in i, b in j} |(ab|ab)|)
+// over the Cartesian functions of the pair (the quantity PySCF's
+// CVHFsetnr_direct_scf gives the reference, cuobc/scf/hf.py:341).
+// One thread per shell pair, bra shell of the larger l.
+// ---------------------------------------------------------------------------
+template <int LI, int LJ>
+__global__ void jk_qcond_kernel(const int* __restrict__ pi, const int* __restrict__ pj, int npairs,
+                                const int* __restrict__ atm, const int* __restrict__ bas,
+                                const double* __restrict__ env, int nbas, double* __restrict__ q) {
+    using C = JKClass<LI, LJ, LI, LJ>;
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npairs) return;
+    int ish = pi[p], jsh = pj[p];
+    const double* ri = env + atm[bas[ish * BAS_SLOTS + ATOM_OF] * ATM_SLOTS + PTR_COORD];
+    const double* rj = env + atm[bas[jsh * BAS_SLOTS + ATOM_OF] * ATM_SLOTS + PTR_COORD];
+    int npi = bas[ish * BAS_SLOTS + NPRIM_OF], npj = bas[jsh * BAS_SLOTS + NPRIM_OF];
+    const double* ai = env + bas[ish * BAS_SLOTS + PTR_EXP];
+    const double* aj = env + bas[jsh * BAS_SLOTS + PTR_EXP];
+    const double* ci = env + bas[ish * BAS_SLOTS + PTR_COEFF];
+    const double* cj = env + bas[jsh * BAS_SLOTS + PTR_COEFF];
+    double fsp = (LI == 0 ? 0.282094791773878143 : (LI == 1 ? 0.488602511902919921 : 1.0)) *
+                 (LJ == 0 ? 0.282094791773878143 : (LJ == 1 ? 0.488602511902919921 : 1.0));
+    double r2 = 0;
+    for (int d = 0; d < 3; d++) r2 += (ri[d] - rj[d]) * (ri[d] - rj[d]);
+    double diag[C::NFI * C::NFJ];
+#pragma unroll
+    for (int e = 0; e < C::NFI * C::NFJ; e++) diag[e] = 0;
+    double r_i[3] = {ri[0], ri[1], ri[2]}, r_j[3] = {rj[0], rj[1], rj[2]};
+    for (int ip = 0; ip < npi; ip++)
+        for (int jp = 0; jp < npj; jp++) {
+            double A = ai[ip] + aj[jp];
+            double eij = fsp * ci[ip] * cj[jp] * exp(-r2 * ai[ip] * aj[jp] / A);
+            double P[3];
+            for (int d = 0; d < 3; d++) P[d] = (ai[ip] * ri[d] + aj[jp] * rj[d]) / A;
+            for (int kp = 0; kp < npi; kp++)
+                for (int lp = 0; lp < npj; lp++) {
+                    double B = ai[kp] + aj[lp];
+                    double ekl = fsp * ci[kp] * cj[lp] * exp(-r2 * ai[kp] * aj[lp] / B);
+                    JKPrim pr;
+                    pr.A = A;
+                    pr.B = B;
+                    pr.AB = A + B;
+                    for (int d = 0; d < 3; d++) {
+                        pr.P[d] = P[d];
+                        pr.Q[d] = (ai[kp] * ri[d] + aj[lp] * rj[d]) / B;
+                    }
+                    double dx = pr.P[0] - pr.Q[0], dy = pr.P[1] - pr.Q[1], dz = pr.P[2] - pr.Q[2];
+                    pr.x = A * B / pr.AB * (dx * dx + dy * dy + dz * dz);
+                    pr.sy = eij * ekl / (sqrt(pr.AB) * A * B);
+                    for (int r = 0; r < C::NROOTS; r++) {
+                        double s, w;
+                        rys_root<C::NROOTS>(pr.x, r, s, w);
+                        double Ix[C::GS], Iy[C::GS], Iz[C::GS];
+                        jk_unit<C, double>(pr, s, w, 0, 11.13665599366341569, r_i, r_j, r_i, r_j, Ix);
+                        jk_unit<C, double>(pr, s, w, 1, 11.13665599366341569, r_i, r_j, r_i, r_j, Iy);
+                        jk_unit<C, double>(pr, s, w, 2, 11.13665599366341569, r_i, r_j, r_i, r_j, Iz);
+#pragma unroll
+                        for (int a = 0; a < C::NFI; a++)
+#pragma unroll
+                            for (int b = 0; b < C::NFJ; b++) {
+                                int ox = cart_lx(LI, a) * (C::SI + C::SK) + cart_lx(LJ, b) * (C::SJ + 1);
+                                int oy = cart_ly(LI, a) * (C::SI + C::SK) + cart_ly(LJ, b) * (C::SJ + 1);
+                                int oz = cart_lz(LI, a) * (C::SI + C::SK) + cart_lz(LJ, b) * (C::SJ + 1);
+                                diag[a * C::NFJ + b] += Ix[ox] * Iy[oy] * Iz[oz];
+                            }
+                    }
+                }
+        }
+    double mx = 0;
+#pragma unroll
+    for (int e = 0; e < C::NFI * C::NFJ; e++) mx = fmax(mx, fabs(diag[e]));
+    double v = sqrt(mx);
+    q[(size_t)ish * nbas + jsh] = v;
+    q[(size_t)jsh * nbas + ish] = v;
+}
+
+typedef void (*qcond_fn)(const int*, const int*, int, const int*, const int*, const double*, int, double*,
+                         cudaStream_t);
+template <int LI, int LJ>
+static void qcond_launch(const int* pi, const int* pj, int n, const int* atm, const int* bas, const double* env,
+                         int nbas, double* q, cudaStream_t st) {
+    if (n > 0) jk_qcond_kernel<LI, LJ><<<(n + 63) / 64, 64, 0, st>>>(pi, pj, n, atm, bas, env, nbas, q);
+}
+static qcond_fn g_qcond[4][4] = {
+    {qcond_launch<0, 0>, nullptr, nullptr, nullptr},
+    {qcond_launch<1, 0>, qcond_launch<1, 1>, nullptr, nullptr},
+    {qcond_launch<2, 0>, qcond_launch<2, 1>, qcond_launch<2, 2>, nullptr},
+    {qcond_launch<3, 0>, qcond_launch<3, 1>, qcond_launch<3, 2>, qcond_launch<3, 3>},
+};
+
+// ---------------------------------------------------------------------------
+// per-call kernels: density condensation and quartet screening
+// ---------------------------------------------------------------------------
+// dm_cond[gi, gj] = max over the dms of max |D[p, q]|, p in group gi, q in gj
+// (lib.condense('absmax') over the group AO boundaries, cuobc/scf/hf.py:104-107)
+__global__ void jk_dm_cond_kernel(const double* __restrict__ dm, int nao, int n_dm, const int* __restrict__ gao,
+                                  int ngroups, double* __restrict__ out) {
+    int gi = blockIdx.x, gj = blockIdx.y;
+    int p0 = gao[gi], p1 = gao[gi + 1], q0 = gao[gj], q1 = gao[gj + 1];
+    int np = p1 - p0, nq = q1 - q0;
+    double mx = 0;
+    long long n = (long long)np * nq * n_dm;
+    for (long long e = threadIdx.x; e < n; e += blockDim.x) {
+        int idm = (int)(e / ((long long)np * nq));
+        int rem = (int)(e - (long long)idm * np * nq);
+        int p = p0 + rem / nq, qq = q0 + rem % nq;
+        mx = fmax(mx, fabs(dm[(size_t)idm * nao * nao + (size_t)p * nao + qq]));
+    }
+    __shared__ double red[256];
+    red[threadIdx.x] = mx;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[gi * ngroups + gj] = red[0];
+}
+
+struct JKScreenCQ {
+    int cp_ij, cp_kl;
+    int gi, gj, gk, gl;
+    int pair_ij0, n_ij, pair_kl0, n_kl;
+    long long qoff_off;
+};
+
+// One block per class quartet.  Reproduces the reference's screening
+// decision per contracted quartet (cuobc/scf/hf.py:136-145, 567-578 and
+// cuobc/lib/gvhf/nr_jk_driver.cu:252-280):
+//   skip the class quartet if prescreen and max(dm_cond over its 6 group
+//   pairs) < tol; else with scale = nbins / log(min(tol/sub, 0.1)) and
+//   s = floor(scale * log_q), keep (ij, kl) iff s_ij + s_kl < nbins (and
+//   kl <= ij inside a diagonal class quartet).
+// Because log_q is sorted descending inside a class, the kept kl of a row
+// form a prefix; its length is found by binary search and prefix-summed.
+__global__ void jk_screen_kernel(const JKScreenCQ* __restrict__ cqs, const double* __restrict__ log_q,
+                                 const double* __restrict__ dm_cond, int ngroups, double tol, int nbins,
+                                 int prescreen, long long* __restrict__ qoff_all, long long* __restrict__ task0_all) {
+    const JKScreenCQ cq = cqs[blockIdx.x];
+    long long* qoff = qoff_all + cq.qoff_off;
+    const double* c = dm_cond;
+    double sub = fmax(fmax(fmax(c[cq.gi * ngroups + cq.gj], c[cq.gk * ngroups + cq.gl]),
+                           fmax(c[cq.gi * ngroups + cq.gk], c[cq.gj * ngroups + cq.gk])),
+                      fmax(c[cq.gi * ngroups + cq.gl], c[cq.gj * ngroups + cq.gl]));
+    bool skip = prescreen && sub < tol;
+    double cutoff = tol / sub;
+    double scale = nbins / log(fmin(cutoff, 0.1));
+    const double* lq_ij = log_q + cq.pair_ij0;
+    const double* lq_kl = log_q + cq.pair_kl0;
+    bool diag = cq.cp_ij == cq.cp_kl;
+    __shared__ long long carry;
+    __shared__ long long wsum[32];
+    if (threadIdx.x == 0) {
+        carry = 0;
+        qoff[0] = 0;
+    }
+    __syncthreads();
+    for (int base = 0; base < cq.n_ij; base += blockDim.x) {
+        int ij = base + threadIdx.x;
+        long long cnt = 0;
+        if (!skip && ij < cq.n_ij) {
+            int sij = (int)floor(scale * lq_ij[ij]);
+            if (sij < nbins) {
+                int b = nbins - sij;
+                // count kl with floor(scale * lq_kl) < b (non-decreasing in kl)
+                int lo = 0, hi = cq.n_kl;
+                while (lo < hi) {
+                    int mid = (lo + hi) >> 1;
+                    if ((int)floor(scale * lq_kl[mid]) < b) lo = mid + 1; else hi = mid;
+                }
+                cnt = lo;
+                if (diag && cnt > ij + 1) cnt = ij + 1;
+            }
+        }
+        // block inclusive scan of cnt
+        long long v = cnt;
+        int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int o = 1; o < 32; o <<= 1) {
+            long long y = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += y;
+        }
+        if (lane == 31) wsum[warp] = v;
+        __syncthreads();
+        if (warp == 0) {
+            long long w = (lane < (int)(blockDim.x >> 5)) ? wsum[lane] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                long long y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            wsum[lane] = w;
+        }
+        __syncthreads();
+        long long incl = v + (warp ? wsum[warp - 1] : 0) + carry;
+        if (ij < cq.n_ij) qoff[ij + 1] = incl;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = incl;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        task0_all[2 * blockIdx.x] = 0;
+        task0_all[2 * blockIdx.x + 1] = carry;
+    }
+}
+
+// J = 2 (V + V^T), K = V + V^T in place on the working-basis buffers, where
+// V[i, j] = mem[i + nao j]; out_rm[p, q] = fac (mem[p nao + q] + mem[q nao + p])
+__global__ void jk_symmetrize_kernel(const double* __restrict__ in, double* __restrict__ out, int nao, int n_dm,
+                                     double fac) {
+    long long n = (long long)nao * nao * n_dm;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        long long m = e / ((long long)nao * nao);
+        long long r = e - m * nao * nao;
+        int p = (int)(r / nao), q = (int)(r % nao);
+        const double* b = in + m * nao * nao;
+        out[e] = fac * (b[(size_t)p * nao + q] + b[(size_t)q * nao + p]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// basis object
+// ---------------------------------------------------------------------------
+struct jk_basis {
+    int device = 0, nsm = 148;
+    int natm = 0, nbas = 0, nao = 0, ngroups = 0, ncp = 0, ncq = 0;
+    double diag_fac = 0.5, cutoff = 1e-13;
+    std::vector<int> h_ao_loc, h_group_off, h_group_l, h_group_nprim;
+    std::vector<int> h_cls_gi, h_cls_gj, h_pair_locs, h_prim_locs, h_pair2bra, h_pair2ket;
+    std::vector<double> h_log_q, h_qcond;
+    std::vector<JKScreenCQ> h_cq;
+    std::vector<long long> h_qoff_off;
+    long long qoff_total = 0;
+    // device
+    int *d_atm = nullptr, *d_bas = nullptr, *d_ao_loc = nullptr, *d_group_ao = nullptr;
+    double *d_env = nullptr, *d_bas_x = nullptr, *d_qcond = nullptr;
+    int *d_pair2bra = nullptr, *d_pair2ket = nullptr;
+    double *d_log_q = nullptr, *d_prim = nullptr;  // prim: a12|e12|x12|y12|z12
+    long long nprim_total = 0;
+    JKScreenCQ* d_cq = nullptr;
+    long long *d_qoff = nullptr, *d_task0 = nullptr;
+    double* d_dm_cond = nullptr;
+    JKSeg* d_seg = nullptr;
+    JKSeg* h_seg = nullptr;  // pinned
+    // reference-compatible single class-pair path
+    long long* d_qoff1 = nullptr;
+    long long* d_task01 = nullptr;
+    long long qoff1_cap = 0;
+    long long* h_qoff1 = nullptr;  // pinned
+    size_t h_qoff1_cap = 0;
+    JKSeg* d_seg1 = nullptr;
+    JKSeg* h_seg1 = nullptr;
+    // transform workspace
+    cublasHandle_t blas = nullptr;
+    double* d_work = nullptr;
+    size_t work_cap = 0;
+};
+
+static void free_basis(jk_basis* b) {
+    if (!b) return;
+    cudaFree(b->d_atm);
+    cudaFree(b->d_bas);
+    cudaFree(b->d_ao_loc);
+    cudaFree(b->d_group_ao);
+    cudaFree(b->d_env);
+    cudaFree(b->d_bas_x);
+    cudaFree(b->d_qcond);
+    cudaFree(b->d_pair2bra);
+    cudaFree(b->d_pair2ket);
+    cudaFree(b->d_log_q);
+    cudaFree(b->d_prim);
+    cudaFree(b->d_cq);
+    cudaFree(b->d_qoff);
+    cudaFree(b->d_task0);
+    cudaFree(b->d_dm_cond);
+    cudaFree(b->d_seg);
+    cudaFree(b->d_qoff1);
+    cudaFree(b->d_task01);
+    cudaFree(b->d_seg1);
+    cudaFree(b->d_work);
+    if (b->h_seg) cudaFreeHost(b->h_seg);
+    if (b->h_seg1) cudaFreeHost(b->h_seg1);
+    if (b->h_qoff1) cudaFreeHost(b->h_qoff1);
+    if (b->blas) cublasDestroy(b->blas);
+    delete b;
+}
+
+template <typename T>
+static cudaError_t upload(T** dst, const T* src, size_t n) {
+    cudaError_t e = cudaMalloc((void**)dst, sizeof(T) * (n ? n : 1));
+    if (e != cudaSuccess) return e;
+    if (n) e = cudaMemcpy(*dst, src, sizeof(T) * n, cudaMemcpyHostToDevice);
+    return e;
+}
+
+extern "C" int jk_rys_table_uniform(void);
+
+static int create_impl(const int* atm, int natm, const int* bas, int nbas, const double* env, int nenv,
+                       const int* group_off, int ngroups, double cutoff, int diag_block_with_triu, jk_basis* b) {
+    init_tables();
+    if (!jk_rys_table_uniform()) return set_err(JK_ERR_ARG, "Rys tables must use intervals of width 2");
+    CUDA_TRY(cudaGetDevice(&b->device));
+    CUDA_TRY(cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, b->device));
+    b->natm = natm;
+    b->nbas = nbas;
+    b->ngroups = ngroups;
+    b->cutoff = cutoff;
+    b->diag_fac = diag_block_with_triu ? 1.0 : 0.5;
+    // shells must be sorted into groups of equal (l, nprim), one contraction each
+    b->h_group_off.assign(group_off, group_off + ngroups + 1);
+    if (b->h_group_off[0] != 0 || b->h_group_off[ngroups] != nbas)
+        return set_err(JK_ERR_ARG, "group offsets must span 0..nbas");
+    b->h_ao_loc.resize(nbas + 1);
+    b->h_ao_loc[0] = 0;
+    for (int i = 0; i < nbas; i++) {
+        int l = bas[i * BAS_SLOTS + ANG_OF];
+        if (l < 0 || l > JK_LMAX)
+            return set_err(JK_ERR_UNSUPPORTED, "shell %d has l=%d; this engine handles l <= %d", i, l, JK_LMAX);
+        if (bas[i * BAS_SLOTS + NCTR_OF] != 1)
+            return set_err(JK_ERR_ARG, "shell %d: generally contracted shells must be split first", i);
+        b->h_ao_loc[i + 1] = b->h_ao_loc[i] + (l + 1) * (l + 2) / 2;
+    }
+    b->nao = b->h_ao_loc[nbas];
+    for (int g = 0; g < ngroups; g++) {
+        int s0 = group_off[g], s1 = group_off[g + 1];
+        if (s1 <= s0) return set_err(JK_ERR_ARG, "empty group %d", g);
+        int l = bas[s0 * BAS_SLOTS + ANG_OF], np = bas[s0 * BAS_SLOTS + NPRIM_OF];
+        for (int s = s0; s < s1; s++)
+            if (bas[s * BAS_SLOTS + ANG_OF] != l || bas[s * BAS_SLOTS + NPRIM_OF] != np)
+                return set_err(JK_ERR_ARG, "group %d mixes (l, nprim)", g);
+        if (g > 0 && l < b->h_group_l[g - 1]) return set_err(JK_ERR_ARG, "groups must be sorted by l");
+        b->h_group_l.push_back(l);
+        b->h_group_nprim.push_back(np);
+    }
+    // device copies of the basis
+    CUDA_TRY(upload(&b->d_atm, atm, (size_t)natm * ATM_SLOTS));
+    CUDA_TRY(upload(&b->d_bas, bas, (size_t)nbas * BAS_SLOTS));
+    CUDA_TRY(upload(&b->d_env, env, (size_t)nenv));
+    CUDA_TRY(upload(&b->d_ao_loc, b->h_ao_loc.data(), b->h_ao_loc.size()));
+    std::vector<int> gao(ngroups + 1);
+    for (int g = 0; g <= ngroups; g++) gao[g] = b->h_ao_loc[group_off[g]];
+    CUDA_TRY(upload(&b->d_group_ao, gao.data(), gao.size()));
+    std::vector<double> bx(3 * (size_t)nbas);
+    for (int i = 0; i < nbas; i++) {
+        const double* r = env + atm[bas[i * BAS_SLOTS + ATOM_OF] * ATM_SLOTS + PTR_COORD];
+        bx[i] = r[0];
+        bx[nbas + i] = r[1];
+        bx[2 * (size_t)nbas + i] = r[2];
+    }
+    CUDA_TRY(upload(&b->d_bas_x, bx.data(), bx.size()));
+
+    // Schwarz matrix on the device
+    CUDA_TRY(cudaMalloc(&b->d_qcond, sizeof(double) * (size_t)nbas * nbas));
+    CUDA_TRY(cudaMemset(b->d_qcond, 0, sizeof(double) * (size_t)nbas * nbas));
+    {
+        std::vector<int> pi[4][4], pj[4][4];
+        for (int i = 0; i < nbas; i++)
+            for (int j = 0; j <= i; j++) {
+                int li = bas[i * BAS_SLOTS + ANG_OF], lj = bas[j * BAS_SLOTS + ANG_OF];
+                if (li >= lj) { pi[li][lj].push_back(i); pj[li][lj].push_back(j); }
+                else { pi[lj][li].push_back(j); pj[lj][li].push_back(i); }
+            }
+        for (int a = 0; a < 4; a++)
+            for (int c = 0; c <= a; c++) {
+                int n = (int)pi[a][c].size();
+                if (!n) continue;
+                int *dpi, *dpj;
+                CUDA_TRY(upload(&dpi, pi[a][c].data(), n));
+                CUDA_TRY(upload(&dpj, pj[a][c].data(), n));
+                g_qcond[a][c](dpi, dpj, n, b->d_atm, b->d_bas, b->d_env, nbas, b->d_qcond, 0);
+                cudaError_t e = cudaGetLastError();
+                if (e == cudaSuccess) e = cudaDeviceSynchronize();
+                cudaFree(dpi);
+                cudaFree(dpj);
+                CUDA_TRY(e);
+            }
+        b->h_qcond.resize((size_t)nbas * nbas);
+        CUDA_TRY(cudaMemcpy(b->h_qcond.data(), b->d_qcond, sizeof(double) * (size_t)nbas * nbas,
+                            cudaMemcpyDeviceToHost));
+    }
+    // Schwarz-sorted pair lists per lower-triangular group pair, in the
+    // reference's class order (cuobc/scf/hf.py:343-389)
+    const std::vector<double>& q = b->h_qcond;
+    b->h_pair_locs.push_back(0);
+    for (int gi = 0; gi < ngroups; gi++) {
+        for (int gj = 0; gj <= gi; gj++) {
+            std::vector<std::pair<double, long long>> lst;
+            int p0 = group_off[gi], p1 = group_off[gi + 1], q0 = group_off[gj], q1 = group_off[gj + 1];
+            for (int i = p0; i < p1; i++)
+                for (int j = q0; j < q1; j++) {
+                    if (gi == gj && !diag_block_with_triu && j > i) continue;
+                    double v = q[(size_t)i * nbas + j];
+                    if (v > cutoff) lst.push_back({v, (long long)i * nbas + j});
+                }
+            std::stable_sort(lst.begin(), lst.end(),
+                             [](const std::pair<double, long long>& x, const std::pair<double, long long>& y) {
+                                 return x.first > y.first;
+                             });
+            for (auto& e : lst) {
+                b->h_pair2bra.push_back((int)(e.second / nbas));
+                b->h_pair2ket.push_back((int)(e.second % nbas));
+                double lq = log(e.first);
+                b->h_log_q.push_back(lq > 0 ? 0 : lq);
+            }
+            b->h_cls_gi.push_back(gi);
+            b->h_cls_gj.push_back(gj);
+            b->h_pair_locs.push_back((int)b->h_pair2bra.size());
+        }
+    }
+    b->ncp = (int)b->h_cls_gi.size();
+    // primitive-pair data (cuobc/lib/gint/pair_data.c:83-141)
+    long long npp = 0;
+    b->h_prim_locs.push_back(0);
+    for (int c = 0; c < b->ncp; c++) {
+        int np12 = b->h_group_nprim[b->h_cls_gi[c]] * b->h_group_nprim[b->h_cls_gj[c]];
+        npp += (long long)(b->h_pair_locs[c + 1] - b->h_pair_locs[c]) * np12;
+        if (npp > 0x7fffffffLL) return set_err(JK_ERR_ARG, "too many primitive pairs");
+        b->h_prim_locs.push_back((int)npp);
+    }
+    b->nprim_total = npp;
+    std::vector<double> prim(5 * (size_t)(npp ? npp : 1));
+    double *a12 = prim.data(), *e12 = a12 + npp, *x12 = e12 + npp, *y12 = x12 + npp, *z12 = y12 + npp;
+    {
+        long long off = 0;
+        for (size_t p = 0; p < b->h_pair2bra.size(); p++) {
+            int ish = b->h_pair2bra[p], jsh = b->h_pair2ket[p];
+            int npi = bas[ish * BAS_SLOTS + NPRIM_OF], npj = bas[jsh * BAS_SLOTS + NPRIM_OF];
+            int li = bas[ish * BAS_SLOTS + ANG_OF], lj = bas[jsh * BAS_SLOTS + ANG_OF];
+            const double* ai = env + bas[ish * BAS_SLOTS + PTR_EXP];
+            const double* aj = env + bas[jsh * BAS_SLOTS + PTR_EXP];
+            const double* ci = env + bas[ish * BAS_SLOTS + PTR_COEFF];
+            const double* cj = env + bas[jsh * BAS_SLOTS + PTR_COEFF];
+            const double* ri = env + atm[bas[ish * BAS_SLOTS + ATOM_OF] * ATM_SLOTS + PTR_COORD];
+            const double* rj = env + atm[bas[jsh * BAS_SLOTS + ATOM_OF] * ATM_SLOTS + PTR_COORD];
+            double norm = common_fac_sp(li) * common_fac_sp(lj);
+            double dx = ri[0] - rj[0], dy = ri[1] - rj[1], dz = ri[2] - rj[2];
+            double r2 = dx * dx + dy * dy + dz * dz;
+            for (int ip = 0; ip < npi; ip++)
+                for (int jp = 0; jp < npj; jp++, off++) {
+                    double aij = ai[ip] + aj[jp];
+                    a12[off] = aij;
+                    e12[off] = norm * ci[ip] * cj[jp] * exp(-r2 * ai[ip] * aj[jp] / aij);
+                    if (ish == jsh) e12[off] *= b->diag_fac;
+                    x12[off] = (ai[ip] * ri[0] + aj[jp] * rj[0]) / aij;
+                    y12[off] = (ai[ip] * ri[1] + aj[jp] * rj[1]) / aij;
+                    z12[off] = (ai[ip] * ri[2] + aj[jp] * rj[2]) / aij;
+                }
+        }
+    }
+    CUDA_TRY(upload(&b->d_prim, prim.data(), prim.size()));
+    CUDA_TRY(upload(&b->d_pair2bra, b->h_pair2bra.data(), b->h_pair2bra.size()));
+    CUDA_TRY(upload(&b->d_pair2ket, b->h_pair2ket.data(), b->h_pair2ket.size()));
+    CUDA_TRY(upload(&b->d_log_q, b->h_log_q.data(), b->h_log_q.size()));
+    // class quartets (cp_ij >= cp_kl), each with its slice of the qoff buffer
+    for (int cij = 0; cij < b->ncp; cij++)
+        for (int ckl = 0; ckl <= cij; ckl++) {
+            JKScreenCQ c;
+            c.cp_ij = cij;
+            c.cp_kl = ckl;
+            c.gi = b->h_cls_gi[cij];
+            c.gj = b->h_cls_gj[cij];
+            c.gk = b->h_cls_gi[ckl];
+            c.gl = b->h_cls_gj[ckl];
+            c.pair_ij0 = b->h_pair_locs[cij];
+            c.n_ij = b->h_pair_locs[cij + 1] - c.pair_ij0;
+            c.pair_kl0 = b->h_pair_locs[ckl];
+            c.n_kl = b->h_pair_locs[ckl + 1] - c.pair_kl0;
+            if (c.n_ij == 0 || c.n_kl == 0) continue;
+            c.qoff_off = b->qoff_total;
+            b->qoff_total += c.n_ij + 1;
+            b->h_cq.push_back(c);
+        }
+    b->ncq = (int)b->h_cq.size();
+    CUDA_TRY(upload(&b->d_cq, b->h_cq.data(), b->h_cq.size()));
+    CUDA_TRY(cudaMalloc(&b->d_qoff, sizeof(long long) * (b->qoff_total ? b->qoff_total : 1)));
+    CUDA_TRY(cudaMalloc(&b->d_task0, sizeof(long long) * 2 * (b->ncq ? b->ncq : 1)));
+    CUDA_TRY(cudaMalloc(&b->d_dm_cond, sizeof(double) * ngroups * ngroups));
+    CUDA_TRY(cudaMalloc(&b->d_seg, sizeof(JKSeg) * (b->ncq ? b->ncq : 1)));
+    CUDA_TRY(cudaMallocHost(&b->h_seg, sizeof(JKSeg) * (b->ncq ? b->ncq : 1)));
+    CUDA_TRY(cudaMalloc(&b->d_seg1, sizeof(JKSeg)));
+    CUDA_TRY(cudaMallocHost(&b->h_seg1, sizeof(JKSeg)));
+    CUDA_TRY(cudaMalloc(&b->d_task01, sizeof(long long) * 2));
+    return JK_OK;
+}
+
+extern "C" int jk_basis_create(const int* atm, int natm, const int* bas, int nbas, const double* env, int nenv,
+                               const int* group_offsets, int ngroups, double cutoff, int diag_block_with_triu,
+                               jk_basis_t** out) {
+    if (!atm || !bas || !env || !group_offsets || !out || natm <= 0 || nbas <= 0 || ngroups <= 0)
+        return set_err(JK_ERR_ARG, "jk_basis_create: invalid arguments");
+    jk_basis* b = new jk_basis();
+    int rc = create_impl(atm, natm, bas, nbas, env, nenv, group_offsets, ngroups, cutoff, diag_block_with_triu, b);
+    if (rc != JK_OK) {
+        free_basis(b);
+        *out = nullptr;
+        return rc;
+    }
+    *out = b;
+    return JK_OK;
+}
+
+extern "C" int jk_basis_destroy(jk_basis_t* b) {
+    free_basis(b);
+    return JK_OK;
+}
+
+extern "C" int jk_basis_info(const jk_basis_t* b, int* info) {
+    if (!b || !info) return set_err(JK_ERR_ARG, "jk_basis_info: invalid arguments");
+    info[0] = b->nbas;
+    info[1] = b->nao;
+    info[2] = b->ngroups;
+    info[3] = b->ncp;
+    info[4] = (int)b->h_pair2bra.size();
+    info[5] = (int)b->nprim_total;
+    info[6] = b->ncq;
+    return JK_OK;
+}
+
+extern "C" int jk_basis_pairs(const jk_basis_t* b, int* pair2shls, int* pair_locs, double* log_q, double* q_cond) {
+    if (!b) return set_err(JK_ERR_ARG, "jk_basis_pairs: null basis");
+    size_t np = b->h_pair2bra.size();
+    if (pair2shls) {
+        std::copy(b->h_pair2bra.begin(), b->h_pair2bra.end(), pair2shls);
+        std::copy(b->h_pair2ket.begin(), b->h_pair2ket.end(), pair2shls + np);
+    }
+    if (pair_locs) std::copy(b->h_pair_locs.begin(), b->h_pair_locs.end(), pair_locs);
+    if (log_q) std::copy(b->h_log_q.begin(), b->h_log_q.end(), log_q);
+    if (q_cond) std::copy(b->h_qcond.begin(), b->h_qcond.end(), q_cond);
+    return JK_OK;
+}
+
+static void fill_seg(const jk_basis* b, int cp_ij, int cp_kl, const long long* qoff, int n_ij, const double* dm,
+                     int n_dm, double* vj, double* vk, JKSeg* s) {
+    s->qoff = qoff;
+    s->n_ij = n_ij;
+    s->pair_ij0 = b->h_pair_locs[cp_ij];
+    s->pair_kl0 = b->h_pair_locs[cp_kl];
+    s->prim_ij0 = b->h_prim_locs[cp_ij];
+    s->prim_kl0 = b->h_prim_locs[cp_kl];
+    s->nprim_ij = b->h_group_nprim[b->h_cls_gi[cp_ij]] * b->h_group_nprim[b->h_cls_gj[cp_ij]];
+    s->nprim_kl = b->h_group_nprim[b->h_cls_gi[cp_kl]] * b->h_group_nprim[b->h_cls_gj[cp_kl]];
+    s->nao = b->nao;
+    s->n_dm = n_dm;
+    s->pair2bra = b->d_pair2bra;
+    s->pair2ket = b->d_pair2ket;
+    long long n = b->nprim_total;
+    s->a12 = b->d_prim;
+    s->e12 = b->d_prim + n;
+    s->x12 = b->d_prim + 2 * n;
+    s->y12 = b->d_prim + 3 * n;
+    s->z12 = b->d_prim + 4 * n;
+    s->bas_x = b->d_bas_x;
+    s->nbas = b->nbas;
+    s->ao_loc = b->d_ao_loc;
+    s->dm = dm;
+    s->vj = vj;
+    s->vk = vk;
+}
+
+static int class_index(const jk_basis* b, int cp_ij, int cp_kl) {
+    int li = b->h_group_l[b->h_cls_gi[cp_ij]], lj = b->h_group_l[b->h_cls_gj[cp_ij]];
+    int lk = b->h_group_l[b->h_cls_gi[cp_kl]], ll = b->h_group_l[b->h_cls_gj[cp_kl]];
+    return li * 64 + lj * 16 + lk * 4 + ll;
+}
+
+extern "C" int jk_build(jk_basis_t* b, const double* dm, int n_dm, double* vj, double* vk, const jk_opts_t* opts,
+                        void* stream) {
+    if (!b || !dm || n_dm <= 0) return set_err(JK_ERR_ARG, "jk_build: invalid arguments");
+    if (!vj && !vk) return JK_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    double tol = opts ? opts->direct_scf_tol : b->cutoff;
+    int nbins = opts && opts->nbins > 0 ? opts->nbins : 10;
+    int prescreen = opts ? opts->prescreen : 1;
+    dim3 gg(b->ngroups, b->ngroups);
+    jk_dm_cond_kernel<<<gg, 256, 0, st>>>(dm, b->nao, n_dm, b->d_group_ao, b->ngroups, b->d_dm_cond);
+    CUDA_TRY(cudaGetLastError());
+    if (b->ncq == 0) return JK_OK;
+    jk_screen_kernel<<<b->ncq, 256, 0, st>>>(b->d_cq, b->d_log_q, b->d_dm_cond, b->ngroups, tol, nbins, prescreen,
+                                            b->d_qoff, b->d_task0);
+    CUDA_TRY(cudaGetLastError());
+    for (int c = 0; c < b->ncq; c++) {
+        const JKScreenCQ& cq = b->h_cq[c];
+        fill_seg(b, cq.cp_ij, cq.cp_kl, b->d_qoff + cq.qoff_off, cq.n_ij, dm, n_dm, vj, vk, b->h_seg + c);
+    }
+    CUDA_TRY(cudaMemcpyAsync(b->d_seg, b->h_seg, sizeof(JKSeg) * b->ncq, cudaMemcpyHostToDevice, st));
+    for (int c = 0; c < b->ncq; c++) {
+        const JKScreenCQ& cq = b->h_cq[c];
+        long long maxt = cq.cp_ij == cq.cp_kl ? (long long)cq.n_ij * (cq.n_ij + 1) / 2
+                                              : (long long)cq.n_ij * cq.n_kl;
+        jk_launch_fn fn = g_tab64[class_index(b, cq.cp_ij, cq.cp_kl)];
+        if (!fn) return set_err(JK_ERR_UNSUPPORTED, "no kernel for class quartet %d", c);
+        CUDA_TRY(fn(b->d_seg + c, b->d_task0 + 2 * c, 1, maxt, b->nsm, st));
+    }
+    // the pinned segment table must not be rewritten before the copy ran
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return JK_OK;
+}
+
+extern "C" int jk_build_class_pair(jk_basis_t* b, double* vj, double* vk, const double* dm, int nao, int n_dm,
+                                   const int* bins_locs_ij, const int* bins_locs_kl, int nbins, int cp_ij,
+                                   int cp_kl, void* stream) {
+    if (!b || !dm || !bins_locs_ij || !bins_locs_kl || nbins <= 0) return set_err(JK_ERR_ARG, "invalid arguments");
+    if (nao != b->nao) return set_err(JK_ERR_ARG, "nao %d does not match the basis (%d)", nao, b->nao);
+    if (cp_ij < 0 || cp_ij >= b->ncp || cp_kl < 0 || cp_kl > cp_ij) return set_err(JK_ERR_ARG, "bad class pair");
+    if (!vj && !vk) return JK_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    int n_ij = b->h_pair_locs[cp_ij + 1] - b->h_pair_locs[cp_ij];
+    // kl bin kb pairs with ij in [bins_ij[0], bins_ij[nbins - kb]) (nr_jk_driver.cu:252-280):
+    // row ij (in bin sij) keeps kl < bins_kl[nbins - sij]; diagonal classes keep kl <= ij
+    if ((size_t)n_ij + 1 > b->h_qoff1_cap) {
+        if (b->h_qoff1) cudaFreeHost(b->h_qoff1);
+        CUDA_TRY(cudaMallocHost(&b->h_qoff1, sizeof(long long) * (n_ij + 1)));
+        b->h_qoff1_cap = n_ij + 1;
+    }
+    CUDA_TRY(cudaStreamSynchronize(st));
+    long long* qo = b->h_qoff1;
+    qo[0] = 0;
+    int sij = 0;
+    long long tot = 0;
+    for (int ij = 0; ij < n_ij; ij++) {
+        while (sij < nbins && ij >= bins_locs_ij[sij + 1]) sij++;
+        long long cnt = 0;
+        if (ij >= bins_locs_ij[0] && sij < nbins) {
+            cnt = bins_locs_kl[nbins - sij] - bins_locs_kl[0];
+            if (bins_locs_kl[0] != 0) cnt = 0;  // the reference's bins always start at 0
+            if (cp_ij == cp_kl && cnt > ij + 1) cnt = ij + 1;
+        }
+        tot += cnt;
+        qo[ij + 1] = tot;
+    }
+    if (n_ij + 1 > b->qoff1_cap) {
+        cudaFree(b->d_qoff1);
+        CUDA_TRY(cudaMalloc(&b->d_qoff1, sizeof(long long) * (n_ij + 1)));
+        b->qoff1_cap = n_ij + 1;
+    }
+    CUDA_TRY(cudaMemcpyAsync(b->d_qoff1, qo, sizeof(long long) * (n_ij + 1), cudaMemcpyHostToDevice, st));
+    long long t0[2] = {0, tot};
+    CUDA_TRY(cudaMemcpyAsync(b->d_task01, t0, sizeof(t0), cudaMemcpyHostToDevice, st));
+    fill_seg(b, cp_ij, cp_kl, b->d_qoff1, n_ij, dm, n_dm, vj, vk, b->h_seg1);
+    CUDA_TRY(cudaMemcpyAsync(b->d_seg1, b->h_seg1, sizeof(JKSeg), cudaMemcpyHostToDevice, st));
+    jk_launch_fn fn = g_tab64[class_index(b, cp_ij, cp_kl)];
+    if (!fn) return set_err(JK_ERR_UNSUPPORTED, "no kernel for this class pair");
+    CUDA_TRY(fn(b->d_seg1, b->d_task01, 1, tot, b->nsm, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return JK_OK;
+}
+
+// row-major C[M,N] = alpha op(A) op(B) + beta C through column-major cuBLAS
+static cublasStatus_t gemm_rm(cublasHandle_t h, bool ta, bool tb, int M, int N, int K, double alpha,
+                              const double* A, int lda, const double* B, int ldb, double beta, double* C, int ldc) {
+    return cublasDgemm(h, tb ? CUBLAS_OP_T : CUBLAS_OP_N, ta ? CUBLAS_OP_T : CUBLAS_OP_N, N, M, K, &alpha, B, ldb,
+                       A, lda, &beta, C, ldc);
+}
+
+#define BLAS_TRY(x)                                                              \
+    do {                                                                         \
+        cublasStatus_t s_ = (x);                                                 \
+        if (s_ != CUBLAS_STATUS_SUCCESS) return set_err(JK_ERR_CUDA, "%s: cublas status %d", #x, (int)s_); \
+    } while (0)
+
+extern "C" int jk_get_jk(jk_basis_t* b, const double* coeff, int nao0, const double* dm0, int n_dm, double* vj0,
+                         double* vk0, const jk_opts_t* opts, void* stream) {
+    if (!b || !coeff || !dm0 || n_dm <= 0 || nao0 <= 0) return set_err(JK_ERR_ARG, "jk_get_jk: invalid arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    int nao = b->nao;
+    size_t nn = (size_t)nao * nao * n_dm;
+    size_t need = 4 * nn + (size_t)nao * nao0;
+    if (need > b->work_cap) {
+        cudaFree(b->d_work);
+        b->d_work = nullptr;
+        CUDA_TRY(cudaMalloc(&b->d_work, sizeof(double) * need));
+        b->work_cap = need;
+    }
+    if (!b->blas) BLAS_TRY(cublasCreate(&b->blas));
+    BLAS_TRY(cublasSetStream(b->blas, st));
+    double* dms = b->d_work;
+    double* vjw = dms + nn;
+    double* vkw = vjw + nn;
+    double* sym = vkw + nn;
+    double* tmp = sym + nn;  // nao x nao0
+    // dms = C D C^T (cuobc/scf/hf.py:73-74)
+    for (int m = 0; m < n_dm; m++) {
+        const double* D = dm0 + (size_t)m * nao0 * nao0;
+        BLAS_TRY(gemm_rm(b->blas, false, false, nao, nao0, nao0, 1.0, coeff, nao0, D, nao0, 0.0, tmp, nao0));
+        BLAS_TRY(gemm_rm(b->blas, false, true, nao, nao, nao0, 1.0, tmp, nao0, coeff, nao0, 0.0,
+                         dms + (size_t)m * nao * nao, nao));
+    }
+    if (vj0) CUDA_TRY(cudaMemsetAsync(vjw, 0, sizeof(double) * nn, st));
+    if (vk0) CUDA_TRY(cudaMemsetAsync(vkw, 0, sizeof(double) * nn, st));
+    int rc = jk_build(b, dms, n_dm, vj0 ? vjw : nullptr, vk0 ? vkw : nullptr, opts, stream);
+    if (rc) return rc;
+    // J = 2 C^T (V + V^T) C, K = C^T (V + V^T) C (cuobc/scf/hf.py:171-181)
+    for (int pass = 0; pass < 2; pass++) {
+        double* out = pass == 0 ? vj0 : vk0;
+        double* w = pass == 0 ? vjw : vkw;
+        if (!out) continue;
+        jk_symmetrize_kernel<<<b->nsm * 4, 256, 0, st>>>(w, sym, nao, n_dm, pass == 0 ? 2.0 : 1.0);
+        CUDA_TRY(cudaGetLastError());
+        for (int m = 0; m < n_dm; m++) {
+            BLAS_TRY(gemm_rm(b->blas, false, false, nao, nao0, nao, 1.0, sym + (size_t)m * nao * nao, nao, coeff,
+                             nao0, 0.0, tmp, nao0));
+            BLAS_TRY(gemm_rm(b->blas, true, false, nao0, nao0, nao, 1.0, coeff, nao0, tmp, nao0, 0.0,
+                             out + (size_t)m * nao0 * nao0, nao0));
+        }
+    }
+    return JK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// introspection for the bench and the tests
+// ---------------------------------------------------------------------------
+// per class quartet: cp_ij, cp_kl, li, lj, lk, ll, nprim_ij, nprim_kl
+extern "C" int jk_basis_cq_info(const jk_basis_t* b, int* out) {
+    if (!b || !out) return set_err(JK_ERR_ARG, "jk_basis_cq_info: invalid arguments");
+    for (int c = 0; c < b->ncq; c++) {
+        const JKScreenCQ& cq = b->h_cq[c];
+        int* o = out + 8 * c;
+        o[0] = cq.cp_ij;
+        o[1] = cq.cp_kl;
+        o[2] = b->h_group_l[cq.gi];
+        o[3] = b->h_group_l[cq.gj];
+        o[4] = b->h_group_l[cq.gk];
+        o[5] = b->h_group_l[cq.gl];
+        o[6] = b->h_group_nprim[cq.gi] * b->h_group_nprim[cq.gj];
+        o[7] = b->h_group_nprim[cq.gk] * b->h_group_nprim[cq.gl];
+    }
+    return JK_OK;
+}
+
+// screened contracted-quartet counts of the last jk_build, per class quartet
+extern "C" int jk_last_counts(const jk_basis_t* b, long long* out, void* stream) {
+    if (!b || !out) return set_err(JK_ERR_ARG, "jk_last_counts: invalid arguments");
+    if (b->ncq == 0) return JK_OK;
+    std::vector<long long> t(2 * (size_t)b->ncq);
+    CUDA_TRY(cudaMemcpyAsync(t.data(), b->d_task0, sizeof(long long) * t.size(), cudaMemcpyDeviceToHost,
+                             (cudaStream_t)stream));
+    CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    for (int c = 0; c < b->ncq; c++) out[c] = t[2 * c + 1];
+    return JK_OK;
+}
+
+// FMA-pipe peak: 8 independent FMA chains per thread, whole device
+template <typename T>
+__global__ void jk_fma_peak_kernel(T* out, int iters) {
+    T a[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) a[k] = (T)(threadIdx.x * 1e-7 + k);
+    const T b = (T)0.9999999, c = (T)1e-7;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+#pragma unroll
+            for (int k = 0; k < 8; k++) a[k] = fma(a[k], b, c);
+        }
+    }
+    T s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) s += a[k];
+    if (s == (T)-1) out[0] = s;  // keeps the chains alive
+}
+
+extern "C" int jk_fma_peak(int fp32, double* tflops) {
+    if (!tflops) return set_err(JK_ERR_ARG, "jk_fma_peak: null output");
+    int dev, nsm;
+    CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    void* buf;
+    CUDA_TRY(cudaMalloc(&buf, 16));
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    const int iters = 4096, threads = 256, blocks = nsm * 8;
+    double best = 0;
+    for (int rep = 0; rep < 4; rep++) {
+        CUDA_TRY(cudaEventRecord(e0));
+        if (fp32) jk_fma_peak_kernel<float><<<blocks, threads>>>((float*)buf, iters);
+        else jk_fma_peak_kernel<double><<<blocks, threads>>>((double*)buf, iters);
+        CUDA_TRY(cudaEventRecord(e1));
+        CUDA_TRY(cudaEventSynchronize(e1));
+        float ms;
+        CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+        double flops = 2.0 * 8 * 16 * (double)iters * threads * blocks;
+        if (rep > 0 && flops / (ms * 1e-3) / 1e12 > best) best = flops / (ms * 1e-3) / 1e12;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(buf);
+    *tflops = best;
+    return JK_OK;
+}

@@ -1,0 +1,24 @@
+// Instantiations of the J/K launchers (one file per slice of classes so
+// the build compiles them in parallel).
+#include "jk_launch.cuh"
+
+void jk_register_l2(jk_launch_fn* tab64, jk_launch_fn* tab32) {
+    JK_REG(2, 0, 0, 0)
+    JK_REG(2, 0, 1, 0)
+    JK_REG(2, 0, 1, 1)
+    JK_REG(2, 0, 2, 0)
+    JK_REG(2, 0, 2, 1)
+    JK_REG(2, 0, 2, 2)
+    JK_REG(2, 1, 0, 0)
+    JK_REG(2, 1, 1, 0)
+    JK_REG(2, 1, 1, 1)
+    JK_REG(2, 1, 2, 0)
+    JK_REG(2, 1, 2, 1)
+    JK_REG(2, 1, 2, 2)
+    JK_REG(2, 2, 0, 0)
+    JK_REG(2, 2, 1, 0)
+    JK_REG(2, 2, 1, 1)
+    JK_REG(2, 2, 2, 0)
+    JK_REG(2, 2, 2, 1)
+    JK_REG(2, 2, 2, 2)
+}

@@ -1,0 +1,508 @@
+// J/K kernels: Rys-quadrature ERIs of contracted shell quartets digested on
+// the fly into J and K (the work of the reference's GINTint2e_jk_kernel*,
+// cuobc/lib/gvhf/g2e.cu:998-1605, and GINTkernel_getjk,
+// cuobc/lib/gvhf/contract_jk.cu:28-635).
+//
+// Work unit: one screened contracted shell quartet (ij|kl) of one segment.
+// All primitive quartets and roots of it are summed in registers before the
+// quartet's contribution to J and K is formed, so every J/K element of the
+// quartet is written with one atomic, instead of one per primitive and root.
+//
+// Two execution shapes, fixed per class at compile time (JKClass::P):
+//   P = 0  one thread per quartet; the 2D integrals of one root live in
+//          registers and all NF Cartesian products accumulate in registers;
+//          the digestion goes straight to global atomics;
+//   P > 0  a team of T threads per quartet: the 3*NROOTS (axis, root) 2D
+//          blocks are built cooperatively in shared memory, each thread owns
+//          the leading P Cartesian indices (i, or i and j) and accumulates the
+//          remaining components in registers; the digestion reduces the
+//          partial J/K blocks of the team in shared memory and flushes each
+//          element with one global atomic.
+// R is the arithmetic type of the recursion and products (double, or float
+// for the mixed-precision path); roots, weights, prefactors and all J/K
+// accumulation stay in double.
+#pragma once
+#include "jk_common.cuh"
+
+__device__ __forceinline__ int jk_find_seg(const long long* __restrict__ task0, int nseg, long long t) {
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (task0[mid] <= t) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int jk_find_row(const long long* __restrict__ qoff, int n, long long t) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (__ldg(qoff + mid) <= t) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+struct JKQuartet {
+    int ish, jsh, ksh, lsh;
+    int prim_ij, prim_kl;  // first primitive pair of ij and kl
+    double norm;
+};
+
+__device__ __forceinline__ JKQuartet jk_decode(const JKSeg& sg, long long local) {
+    JKQuartet q;
+    int row = jk_find_row(sg.qoff, sg.n_ij, local);
+    int col = (int)(local - __ldg(sg.qoff + row));
+    int bij = sg.pair_ij0 + row, bkl = sg.pair_kl0 + col;
+    q.ish = __ldg(sg.pair2bra + bij);
+    q.jsh = __ldg(sg.pair2ket + bij);
+    q.ksh = __ldg(sg.pair2bra + bkl);
+    q.lsh = __ldg(sg.pair2ket + bkl);
+    q.prim_ij = sg.prim_ij0 + row * sg.nprim_ij;
+    q.prim_kl = sg.prim_kl0 + col * sg.nprim_kl;
+    // 2 pi^3 / sqrt(pi), halved on the ij == kl diagonal (g2e.c:41, g2e.cu:1025)
+    q.norm = 11.13665599366341569 * (bij == bkl ? 0.5 : 1.0);
+    return q;
+}
+
+// prefactors of one primitive quartet
+struct JKPrim {
+    double x, A, B, AB, sy;  // Boys argument, exponent sums, y seed
+    double P[3], Q[3];
+};
+
+__device__ __forceinline__ JKPrim jk_prim(const JKSeg& sg, int pij, int pkl) {
+    JKPrim p;
+    p.A = __ldg(sg.a12 + pij);
+    p.B = __ldg(sg.a12 + pkl);
+    p.P[0] = __ldg(sg.x12 + pij);
+    p.P[1] = __ldg(sg.y12 + pij);
+    p.P[2] = __ldg(sg.z12 + pij);
+    p.Q[0] = __ldg(sg.x12 + pkl);
+    p.Q[1] = __ldg(sg.y12 + pkl);
+    p.Q[2] = __ldg(sg.z12 + pkl);
+    p.AB = p.A + p.B;
+    double rho = p.A * p.B / p.AB;
+    double dx = p.P[0] - p.Q[0], dy = p.P[1] - p.Q[1], dz = p.P[2] - p.Q[2];
+    p.x = rho * (dx * dx + dy * dy + dz * dz);
+    p.sy = __ldg(sg.e12 + pij) * __ldg(sg.e12 + pkl) / (sqrt(p.AB) * p.A * p.B);
+    return p;
+}
+
+// build the 2D block of (axis d, root r) into out
+template <class C, typename R, typename OutT>
+__device__ __forceinline__ void jk_unit(const JKPrim& p, double s, double w, int d, double norm, const double* ri,
+                                        const double* rj, const double* rk, const double* rl, OutT* out) {
+    // select by d without dynamic indexing (keeps everything in registers)
+#define JK_PICK(a) (d == 0 ? (a)[0] : (d == 1 ? (a)[1] : (a)[2]))
+    double bs = p.B * s / p.AB, as = p.A * s / p.AB;
+    double b00 = 0.5 * s / p.AB;
+    double b10 = 0.5 / p.A * (1. - bs);
+    double b01 = 0.5 / p.B * (1. - as);
+    double Pd = JK_PICK(p.P), Qd = JK_PICK(p.Q);
+    double Rid = JK_PICK(ri), Rjd = JK_PICK(rj), Rkd = JK_PICK(rk), Rld = JK_PICK(rl);
+#undef JK_PICK
+    double pq = Pd - Qd;
+    double c00 = (Pd - Rid) - bs * pq;
+    double c0p = (Qd - Rkd) + as * pq;
+    double seed = d == 0 ? norm : (d == 1 ? p.sy : w);
+    rys_2d<R, C>((R)seed, (R)c00, (R)c0p, (R)b10, (R)b01, (R)b00, (R)(Rid - Rjd), (R)(Rkd - Rld), out);
+}
+
+__device__ __forceinline__ void load_center(const JKSeg& sg, int sh, double* r) {
+    r[0] = __ldg(sg.bas_x + sh);
+    r[1] = __ldg(sg.bas_x + sg.nbas + sh);
+    r[2] = __ldg(sg.bas_x + 2 * sg.nbas + sh);
+}
+
+// D_ab with the reference's index convention dm[a + nao*b]
+#define DM(a, b) __ldg(D + (a) + (size_t)nao * (b))
+
+// ===========================================================================
+// P = 0: one thread per quartet
+// ===========================================================================
+template <class C, typename R>
+__device__ __forceinline__ void jk_thread_quartet(const JKSeg& sg, const JKQuartet& q) {
+    constexpr int NR = C::NROOTS;
+    double ri[3], rj[3], rk[3], rl[3];
+    load_center(sg, q.ish, ri);
+    load_center(sg, q.jsh, rj);
+    load_center(sg, q.ksh, rk);
+    load_center(sg, q.lsh, rl);
+    R acc[C::NF];
+#pragma unroll
+    for (int e = 0; e < C::NF; e++) acc[e] = R(0);
+    for (int ip = 0; ip < sg.nprim_ij; ip++)
+        for (int kp = 0; kp < sg.nprim_kl; kp++) {
+            JKPrim p = jk_prim(sg, q.prim_ij + ip, q.prim_kl + kp);
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                double s, w;
+                rys_root<NR>(p.x, r, s, w);
+                R Ix[C::GS], Iy[C::GS], Iz[C::GS];
+                jk_unit<C, R>(p, s, w, 0, q.norm, ri, rj, rk, rl, Ix);
+                jk_unit<C, R>(p, s, w, 1, q.norm, ri, rj, rk, rl, Iy);
+                jk_unit<C, R>(p, s, w, 2, q.norm, ri, rj, rk, rl, Iz);
+#pragma unroll
+                for (int i = 0; i < C::NFI; i++)
+#pragma unroll
+                    for (int j = 0; j < C::NFJ; j++)
+#pragma unroll
+                        for (int k = 0; k < C::NFK; k++)
+#pragma unroll
+                            for (int l = 0; l < C::NFL; l++) {
+                                int ox = cart_lx(C::LI, i) * C::SI + cart_lx(C::LJ, j) * C::SJ +
+                                         cart_lx(C::LK, k) * C::SK + cart_lx(C::LL, l);
+                                int oy = cart_ly(C::LI, i) * C::SI + cart_ly(C::LJ, j) * C::SJ +
+                                         cart_ly(C::LK, k) * C::SK + cart_ly(C::LL, l);
+                                int oz = cart_lz(C::LI, i) * C::SI + cart_lz(C::LJ, j) * C::SJ +
+                                         cart_lz(C::LK, k) * C::SK + cart_lz(C::LL, l);
+                                acc[((i * C::NFJ + j) * C::NFK + k) * C::NFL + l] += Ix[ox] * Iy[oy] * Iz[oz];
+                            }
+            }
+        }
+    const int nao = sg.nao;
+    const int i0 = __ldg(sg.ao_loc + q.ish), j0 = __ldg(sg.ao_loc + q.jsh);
+    const int k0 = __ldg(sg.ao_loc + q.ksh), l0 = __ldg(sg.ao_loc + q.lsh);
+#define ACC(i, j, k, l) ((double)acc[(((i) * C::NFJ + (j)) * C::NFK + (k)) * C::NFL + (l)])
+    for (int idm = 0; idm < sg.n_dm; idm++) {
+        const double* D = sg.dm + (size_t)idm * nao * nao;
+        if (sg.vj) {
+            double* V = sg.vj + (size_t)idm * nao * nao;
+#pragma unroll
+            for (int i = 0; i < C::NFI; i++)
+#pragma unroll
+                for (int j = 0; j < C::NFJ; j++) {
+                    double v = 0;
+#pragma unroll
+                    for (int k = 0; k < C::NFK; k++)
+#pragma unroll
+                        for (int l = 0; l < C::NFL; l++) v += ACC(i, j, k, l) * DM(k0 + k, l0 + l);
+                    atomicAdd(V + (i0 + i) + (size_t)nao * (j0 + j), v);
+                }
+#pragma unroll
+            for (int k = 0; k < C::NFK; k++)
+#pragma unroll
+                for (int l = 0; l < C::NFL; l++) {
+                    double v = 0;
+#pragma unroll
+                    for (int i = 0; i < C::NFI; i++)
+#pragma unroll
+                        for (int j = 0; j < C::NFJ; j++) v += ACC(i, j, k, l) * DM(i0 + i, j0 + j);
+                    atomicAdd(V + (k0 + k) + (size_t)nao * (l0 + l), v);
+                }
+        }
+        if (sg.vk) {
+            double* V = sg.vk + (size_t)idm * nao * nao;
+#pragma unroll
+            for (int i = 0; i < C::NFI; i++)
+#pragma unroll
+                for (int k = 0; k < C::NFK; k++) {
+                    double v = 0;
+#pragma unroll
+                    for (int j = 0; j < C::NFJ; j++)
+#pragma unroll
+                        for (int l = 0; l < C::NFL; l++) v += ACC(i, j, k, l) * DM(j0 + j, l0 + l);
+                    atomicAdd(V + (i0 + i) + (size_t)nao * (k0 + k), v);
+                }
+#pragma unroll
+            for (int i = 0; i < C::NFI; i++)
+#pragma unroll
+                for (int l = 0; l < C::NFL; l++) {
+                    double v = 0;
+#pragma unroll
+                    for (int j = 0; j < C::NFJ; j++)
+#pragma unroll
+                        for (int k = 0; k < C::NFK; k++) v += ACC(i, j, k, l) * DM(j0 + j, k0 + k);
+                    atomicAdd(V + (i0 + i) + (size_t)nao * (l0 + l), v);
+                }
+#pragma unroll
+            for (int j = 0; j < C::NFJ; j++)
+#pragma unroll
+                for (int k = 0; k < C::NFK; k++) {
+                    double v = 0;
+#pragma unroll
+                    for (int i = 0; i < C::NFI; i++)
+#pragma unroll
+                        for (int l = 0; l < C::NFL; l++) v += ACC(i, j, k, l) * DM(i0 + i, l0 + l);
+                    atomicAdd(V + (j0 + j) + (size_t)nao * (k0 + k), v);
+                }
+#pragma unroll
+            for (int j = 0; j < C::NFJ; j++)
+#pragma unroll
+                for (int l = 0; l < C::NFL; l++) {
+                    double v = 0;
+#pragma unroll
+                    for (int i = 0; i < C::NFI; i++)
+#pragma unroll
+                        for (int k = 0; k < C::NFK; k++) v += ACC(i, j, k, l) * DM(i0 + i, k0 + k);
+                    atomicAdd(V + (j0 + j) + (size_t)nao * (l0 + l), v);
+                }
+        }
+    }
+#undef ACC
+}
+
+template <class C, typename R>
+__global__ void __launch_bounds__(128) jk_thread_kernel(const JKSeg* __restrict__ segs,
+                                                        const long long* __restrict__ task0, int nseg) {
+    long long total = task0[nseg];
+    long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+        int s = jk_find_seg(task0, nseg, t);
+        JKSeg sg = segs[s];
+        JKQuartet q = jk_decode(sg, t - task0[s]);
+        jk_thread_quartet<C, R>(sg, q);
+    }
+}
+
+// ===========================================================================
+// P > 0: a team of T threads per quartet, teams packed into a block
+// ===========================================================================
+template <class C>
+struct JKTeamShape {
+    static constexpr int QPB = (C::T >= 128) ? 1 : (128 / C::T);  // quartets per block
+    static constexpr int THREADS = QPB * C::T;
+    static constexpr int GWORDS = (3 * C::NROOTS * C::GS + 1) & ~1;  // 2D blocks per quartet (even)
+    static constexpr int BWORDS = C::NFI * C::NFJ + C::NFK * C::NFL + C::NFI * C::NFK + C::NFI * C::NFL +
+                                  C::NFJ * C::NFK + C::NFJ * C::NFL;  // digestion buffers
+    static constexpr int OFF_JIJ = 0, OFF_JKL = OFF_JIJ + C::NFI * C::NFJ, OFF_KIK = OFF_JKL + C::NFK * C::NFL,
+                         OFF_KIL = OFF_KIK + C::NFI * C::NFK, OFF_KJK = OFF_KIL + C::NFI * C::NFL,
+                         OFF_KJL = OFF_KJK + C::NFJ * C::NFK;
+};
+
+template <class C, typename R>
+constexpr size_t jk_team_smem() {
+    using S = JKTeamShape<C>;
+    return (size_t)S::QPB * (S::GWORDS * sizeof(R) + S::BWORDS * sizeof(double));
+}
+
+template <class C, typename R>
+__global__ void jk_team_kernel(const JKSeg* __restrict__ segs, const long long* __restrict__ task0, int nseg) {
+    using S = JKTeamShape<C>;
+    constexpr int T = C::T, NR = C::NROOTS;
+    extern __shared__ __align__(16) unsigned char jk_smem[];
+    const int team = threadIdx.x / T, lane = threadIdx.x - team * T;
+    R* g = reinterpret_cast<R*>(jk_smem) + (size_t)team * S::GWORDS;
+    double* buf = reinterpret_cast<double*>(jk_smem + (size_t)S::QPB * S::GWORDS * sizeof(R)) + (size_t)team * S::BWORDS;
+
+    // owned Cartesian indices
+    int ci = 0, cj = 0;
+    if (C::P == 1) ci = lane;
+    if (C::P == 2) {
+        ci = lane / C::NFJ;
+        cj = lane - ci * C::NFJ;
+    }
+    int own_x = cart_lx(C::LI, ci) * C::SI, own_y = cart_ly(C::LI, ci) * C::SI, own_z = cart_lz(C::LI, ci) * C::SI;
+    if (C::P == 2) {
+        own_x += cart_lx(C::LJ, cj) * C::SJ;
+        own_y += cart_ly(C::LJ, cj) * C::SJ;
+        own_z += cart_lz(C::LJ, cj) * C::SJ;
+    }
+
+    const long long total = task0[nseg];
+    const long long nteams = (long long)gridDim.x * S::QPB;
+    const int nprim_ij = segs[0].nprim_ij, nprim_kl = segs[0].nprim_kl;  // uniform within a launch
+    for (long long base = (long long)blockIdx.x * S::QPB; base < total; base += nteams) {
+        const long long t = base + team;
+        const bool active = t < total;
+        JKSeg sg;
+        JKQuartet q;
+        double ri[3], rj[3], rk[3], rl[3];
+        if (active) {
+            int s = jk_find_seg(task0, nseg, t);
+            sg = segs[s];
+            q = jk_decode(sg, t - task0[s]);
+            load_center(sg, q.ish, ri);
+            load_center(sg, q.jsh, rj);
+            load_center(sg, q.ksh, rk);
+            load_center(sg, q.lsh, rl);
+        }
+        R acc[C::NACC];
+#pragma unroll
+        for (int e = 0; e < C::NACC; e++) acc[e] = R(0);
+        for (int ip = 0; ip < nprim_ij; ip++)
+            for (int kp = 0; kp < nprim_kl; kp++) {
+                if (active) {
+                    JKPrim p = jk_prim(sg, q.prim_ij + ip, q.prim_kl + kp);
+                    for (int u = lane; u < 3 * NR; u += T) {
+                        int r = u / 3, d = u - 3 * r;
+                        double s, w;
+                        rys_root<NR>(p.x, r, s, w);
+                        jk_unit<C, R>(p, s, w, d, q.norm, ri, rj, rk, rl, g + u * C::GS);
+                    }
+                }
+                __syncthreads();
+                if (active) {
+#pragma unroll
+                    for (int r = 0; r < NR; r++) {
+                        const R* gx = g + (3 * r) * C::GS;
+                        const R* gy = gx + C::GS;
+                        const R* gz = gy + C::GS;
+                        if (C::P == 1) {
+#pragma unroll
+                            for (int j = 0; j < C::NFJ; j++)
+#pragma unroll
+                                for (int k = 0; k < C::NFK; k++)
+#pragma unroll
+                                    for (int l = 0; l < C::NFL; l++) {
+                                        int ox = cart_lx(C::LJ, j) * C::SJ + cart_lx(C::LK, k) * C::SK + cart_lx(C::LL, l);
+                                        int oy = cart_ly(C::LJ, j) * C::SJ + cart_ly(C::LK, k) * C::SK + cart_ly(C::LL, l);
+                                        int oz = cart_lz(C::LJ, j) * C::SJ + cart_lz(C::LK, k) * C::SK + cart_lz(C::LL, l);
+                                        acc[(j * C::NFK + k) * C::NFL + l] +=
+                                            gx[own_x + ox] * gy[own_y + oy] * gz[own_z + oz];
+                                    }
+                        } else {
+#pragma unroll
+                            for (int k = 0; k < C::NFK; k++)
+#pragma unroll
+                                for (int l = 0; l < C::NFL; l++) {
+                                    int ox = cart_lx(C::LK, k) * C::SK + cart_lx(C::LL, l);
+                                    int oy = cart_ly(C::LK, k) * C::SK + cart_ly(C::LL, l);
+                                    int oz = cart_lz(C::LK, k) * C::SK + cart_lz(C::LL, l);
+                                    acc[k * C::NFL + l] += gx[own_x + ox] * gy[own_y + oy] * gz[own_z + oz];
+                                }
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+
+        // ---- digestion ----
+        const int n_dm = active ? sg.n_dm : segs[0].n_dm;
+        for (int idm = 0; idm < n_dm; idm++) {
+            for (int e = lane; e < S::BWORDS; e += T) buf[e] = 0.;
+            __syncthreads();
+            if (active) {
+                const int nao = sg.nao;
+                const int i0 = __ldg(sg.ao_loc + q.ish), j0 = __ldg(sg.ao_loc + q.jsh);
+                const int k0 = __ldg(sg.ao_loc + q.ksh), l0 = __ldg(sg.ao_loc + q.lsh);
+                const double* D = sg.dm + (size_t)idm * nao * nao;
+                if (C::P == 1) {
+#define A1(j, k, l) ((double)acc[((j) * C::NFK + (k)) * C::NFL + (l)])
+                    const int I = i0 + ci;
+                    if (sg.vj) {
+#pragma unroll
+                        for (int j = 0; j < C::NFJ; j++) {  // J_ij: complete in-thread
+                            double v = 0;
+#pragma unroll
+                            for (int k = 0; k < C::NFK; k++)
+#pragma unroll
+                                for (int l = 0; l < C::NFL; l++) v += A1(j, k, l) * DM(k0 + k, l0 + l);
+                            buf[S::OFF_JIJ + ci * C::NFJ + j] = v;
+                        }
+#pragma unroll
+                        for (int k = 0; k < C::NFK; k++)  // J_kl: reduce over i
+#pragma unroll
+                            for (int l = 0; l < C::NFL; l++) {
+                                double v = 0;
+#pragma unroll
+                                for (int j = 0; j < C::NFJ; j++) v += A1(j, k, l) * DM(I, j0 + j);
+                                atomicAdd(buf + S::OFF_JKL + k * C::NFL + l, v);
+                            }
+                    }
+                    if (sg.vk) {
+#pragma unroll
+                        for (int k = 0; k < C::NFK; k++) {  // K_ik: complete
+                            double v = 0;
+#pragma unroll
+                            for (int j = 0; j < C::NFJ; j++)
+#pragma unroll
+                                for (int l = 0; l < C::NFL; l++) v += A1(j, k, l) * DM(j0 + j, l0 + l);
+                            buf[S::OFF_KIK + ci * C::NFK + k] = v;
+                        }
+#pragma unroll
+                        for (int l = 0; l < C::NFL; l++) {  // K_il: complete
+                            double v = 0;
+#pragma unroll
+                            for (int j = 0; j < C::NFJ; j++)
+#pragma unroll
+                                for (int k = 0; k < C::NFK; k++) v += A1(j, k, l) * DM(j0 + j, k0 + k);
+                            buf[S::OFF_KIL + ci * C::NFL + l] = v;
+                        }
+#pragma unroll
+                        for (int j = 0; j < C::NFJ; j++)
+#pragma unroll
+                            for (int k = 0; k < C::NFK; k++) {  // K_jk: reduce over i
+                                double v = 0;
+#pragma unroll
+                                for (int l = 0; l < C::NFL; l++) v += A1(j, k, l) * DM(I, l0 + l);
+                                atomicAdd(buf + S::OFF_KJK + j * C::NFK + k, v);
+                            }
+#pragma unroll
+                        for (int j = 0; j < C::NFJ; j++)
+#pragma unroll
+                            for (int l = 0; l < C::NFL; l++) {  // K_jl: reduce over i
+                                double v = 0;
+#pragma unroll
+                                for (int k = 0; k < C::NFK; k++) v += A1(j, k, l) * DM(I, k0 + k);
+                                atomicAdd(buf + S::OFF_KJL + j * C::NFL + l, v);
+                            }
+                    }
+#undef A1
+                } else {
+#define A2(k, l) ((double)acc[(k) * C::NFL + (l)])
+                    const int I = i0 + ci, J = j0 + cj;
+                    if (sg.vj) {
+                        double v = 0;  // J_ij: complete
+#pragma unroll
+                        for (int k = 0; k < C::NFK; k++)
+#pragma unroll
+                            for (int l = 0; l < C::NFL; l++) v += A2(k, l) * DM(k0 + k, l0 + l);
+                        buf[S::OFF_JIJ + ci * C::NFJ + cj] = v;
+                        const double dij = DM(I, J);
+#pragma unroll
+                        for (int k = 0; k < C::NFK; k++)
+#pragma unroll
+                            for (int l = 0; l < C::NFL; l++) atomicAdd(buf + S::OFF_JKL + k * C::NFL + l, A2(k, l) * dij);
+                    }
+                    if (sg.vk) {
+#pragma unroll
+                        for (int k = 0; k < C::NFK; k++) {  // K_ik (over j) and K_jk (over i)
+                            double vik = 0, vjk = 0;
+#pragma unroll
+                            for (int l = 0; l < C::NFL; l++) {
+                                vik += A2(k, l) * DM(J, l0 + l);
+                                vjk += A2(k, l) * DM(I, l0 + l);
+                            }
+                            atomicAdd(buf + S::OFF_KIK + ci * C::NFK + k, vik);
+                            atomicAdd(buf + S::OFF_KJK + cj * C::NFK + k, vjk);
+                        }
+#pragma unroll
+                        for (int l = 0; l < C::NFL; l++) {  // K_il (over j) and K_jl (over i)
+                            double vil = 0, vjl = 0;
+#pragma unroll
+                            for (int k = 0; k < C::NFK; k++) {
+                                vil += A2(k, l) * DM(J, k0 + k);
+                                vjl += A2(k, l) * DM(I, k0 + k);
+                            }
+                            atomicAdd(buf + S::OFF_KIL + ci * C::NFL + l, vil);
+                            atomicAdd(buf + S::OFF_KJL + cj * C::NFL + l, vjl);
+                        }
+                    }
+#undef A2
+                }
+            }
+            __syncthreads();
+            if (active) {  // flush the team's blocks to global memory
+                const int nao = sg.nao;
+                const int i0 = __ldg(sg.ao_loc + q.ish), j0 = __ldg(sg.ao_loc + q.jsh);
+                const int k0 = __ldg(sg.ao_loc + q.ksh), l0 = __ldg(sg.ao_loc + q.lsh);
+                const size_t moff = (size_t)idm * nao * nao;
+                for (int e = lane; e < S::BWORDS; e += T) {
+                    double v = buf[e];
+                    double* V;
+                    int a, b;
+                    if (e < S::OFF_JKL) { V = sg.vj; a = i0 + e / C::NFJ; b = j0 + e % C::NFJ; }
+                    else if (e < S::OFF_KIK) { int x = e - S::OFF_JKL; V = sg.vj; a = k0 + x / C::NFL; b = l0 + x % C::NFL; }
+                    else if (e < S::OFF_KIL) { int x = e - S::OFF_KIK; V = sg.vk; a = i0 + x / C::NFK; b = k0 + x % C::NFK; }
+                    else if (e < S::OFF_KJK) { int x = e - S::OFF_KIL; V = sg.vk; a = i0 + x / C::NFL; b = l0 + x % C::NFL; }
+                    else if (e < S::OFF_KJL) { int x = e - S::OFF_KJK; V = sg.vk; a = j0 + x / C::NFK; b = k0 + x % C::NFK; }
+                    else { int x = e - S::OFF_KJL; V = sg.vk; a = j0 + x / C::NFL; b = l0 + x % C::NFL; }
+                    if (V) atomicAdd(V + moff + a + (size_t)nao * b, v);
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+#undef DM

@@ -1,0 +1,46 @@
+// Launchers of the J/K kernels, one per (li, lj, lk, ll) class and arithmetic
+// type, collected in a table indexed by li*64 + lj*16 + lk*4 + ll.
+#pragma once
+#include "jk_kernels.cuh"
+
+typedef cudaError_t (*jk_launch_fn)(const JKSeg* segs, const long long* task0, int nseg, long long max_tasks,
+                                    int nsm, cudaStream_t st);
+
+template <int LI, int LJ, int LK, int LL, typename R>
+cudaError_t jk_launch(const JKSeg* segs, const long long* task0, int nseg, long long max_tasks, int nsm,
+                      cudaStream_t st) {
+    using C = JKClass<LI, LJ, LK, LL>;
+    if (max_tasks <= 0) return cudaSuccess;
+    if constexpr (C::P == 0) {
+        long long want = (max_tasks + 127) / 128;
+        long long cap = (long long)nsm * 16;
+        int blocks = (int)(want < cap ? want : cap);
+        jk_thread_kernel<C, R><<<blocks, 128, 0, st>>>(segs, task0, nseg);
+    } else {
+        using S = JKTeamShape<C>;
+        constexpr size_t smem = jk_team_smem<C, R>();
+        static bool attr_set = false;
+        if (!attr_set) {
+            cudaError_t e = cudaFuncSetAttribute(jk_team_kernel<C, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+            if (e != cudaSuccess) return e;
+            attr_set = true;
+        }
+        long long want = (max_tasks + S::QPB - 1) / S::QPB;
+        long long cap = (long long)nsm * 8;
+        int blocks = (int)(want < cap ? want : cap);
+        jk_team_kernel<C, R><<<blocks, S::THREADS, smem, st>>>(segs, task0, nseg);
+    }
+    return cudaGetLastError();
+}
+
+// per-instantiation-file registration
+void jk_register_l0(jk_launch_fn* tab64, jk_launch_fn* tab32);
+void jk_register_l1(jk_launch_fn* tab64, jk_launch_fn* tab32);
+void jk_register_l2(jk_launch_fn* tab64, jk_launch_fn* tab32);
+void jk_register_l3a(jk_launch_fn* tab64, jk_launch_fn* tab32);
+void jk_register_l3b(jk_launch_fn* tab64, jk_launch_fn* tab32);
+
+#define JK_REG(LI, LJ, LK, LL)                                                     \
+    tab64[(LI)*64 + (LJ)*16 + (LK)*4 + (LL)] = jk_launch<LI, LJ, LK, LL, double>; \
+    tab32[(LI)*64 + (LJ)*16 + (LK)*4 + (LL)] = jk_launch<LI, LJ, LK, LL, float>;

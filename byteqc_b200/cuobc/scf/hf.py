@@ -1,0 +1,259 @@
+"""Direct-SCF J/K on the B200: the host side of ByteQC's ``cuobc`` J/K path.
+
+Same call as the reference (``cuobc/scf/hf.py:53-55``)::
+
+    vj, vk = get_jk(mol, dm, hermi=1, vhfopt=None, with_j=True, with_k=True)
+
+``mol`` is a :class:`byteqc_b200.gto.Mole` (the libcint-layout subset of a
+PySCF ``Mole`` the path reads), ``dm`` a numpy array or a CUDA tensor of
+shape (nao, nao) or (n_dm, nao, nao).  The result has ``dm``'s shape and
+comes back as numpy float64 arrays, as in the reference (``hf.py:176,181``),
+or as CUDA tensors with ``out='device'``.  A disabled matrix is returned as
+``None``.
+
+Everything after the argument checks runs on the GPU through libjk.so: the
+AO transforms, the density condensation, the screening, the Rys J/K kernels
+and the symmetrisation.  There is no CPU fallback.
+"""
+import ctypes
+import math
+
+import numpy as np
+
+from byteqc_b200.cuobc import lib as _lib
+from byteqc_b200.gto import mole as gmole
+
+LMAX_ON_GPU = 3  # f functions; the reference's GPU kernels go up to h
+ANGULAR = 'spdfghik'
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError('the J/K engine needs a CUDA device')
+    return torch
+
+
+def _stream_ptr(torch):
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def basis_seg_contraction(mol):
+    """Working basis of the J/K kernels (cuobc/scf/hf.py:481-564): every
+    generally contracted shell (nctr > 1) is split into its primitive shells,
+    functions are Cartesian, and ``coeff`` (nao_working, nao) maps the
+    working basis back to ``mol``'s contracted (spherical or Cartesian)
+    functions.  Shells with one contraction are kept as they are."""
+    env = mol._env.copy()
+    new_bas = []
+    blocks = []  # (rows, cols) transform block per original shell
+    for shell in mol._bas:
+        l, nprim, nctr = (int(shell[gmole.ANG_OF]), int(shell[gmole.NPRIM_OF]),
+                          int(shell[gmole.NCTR_OF]))
+        nf = gmole.ncart(l)
+        if nctr == 1:
+            new_bas.append(shell.copy())
+            blocks.append(np.eye(nf))
+            continue
+        pexp, pcoeff = int(shell[gmole.PTR_EXP]), int(shell[gmole.PTR_COEFF])
+        exps = env[pexp:pexp + nprim]
+        norm = gmole.gto_norm(l, exps)
+        c = env[pcoeff:pcoeff + nprim * nctr].reshape(nctr, nprim) / norm
+        # rows: (primitive p, component f); cols: (contraction i, component f)
+        blk = np.kron(c.T, np.eye(nf))
+        env[pcoeff:pcoeff + nprim] = norm
+        for p in range(nprim):
+            s = shell.copy()
+            s[gmole.NPRIM_OF] = 1
+            s[gmole.NCTR_OF] = 1
+            s[gmole.PTR_EXP] = pexp + p
+            s[gmole.PTR_COEFF] = pcoeff + p
+            new_bas.append(s)
+        blocks.append(blk)
+    pmol = mol.copy()
+    pmol.cart = True
+    pmol._bas = np.asarray(new_bas, dtype=np.int32).reshape(-1, gmole.BAS_SLOTS)
+    pmol._env = env
+    nrow = sum(b.shape[0] for b in blocks)
+    ncol = sum(b.shape[1] for b in blocks)
+    contr = np.zeros((nrow, ncol))
+    r = c0 = 0
+    for b in blocks:
+        contr[r:r + b.shape[0], c0:c0 + b.shape[1]] = b
+        r += b.shape[0]
+        c0 += b.shape[1]
+    if mol.cart:
+        return pmol, contr
+    return pmol, contr @ mol.cart2sph_coeff()
+
+
+def _split_l_ctr_groups(uniq_l_ctr, l_ctr_counts, group_size):
+    """Cap the AOs per (l, nprim) group (cuobc/scf/hf.py:581-606)."""
+    ls, counts = [], []
+    for l_ctr, cnt in zip(uniq_l_ctr, l_ctr_counts):
+        nf = gmole.ncart(int(l_ctr[0]))
+        max_shells = max(group_size // nf, 2)
+        full, rest = divmod(int(cnt), max_shells) if cnt > max_shells else (0, int(cnt))
+        ls.extend([l_ctr] * (full + (rest > 0)))
+        counts.extend([max_shells] * full + ([rest] if rest else []))
+    return np.vstack(ls), np.asarray(counts)
+
+
+def _make_s_index_offsets(log_q, nbins=10, cutoff=1e-12):
+    """Log-Schwarz bin offsets of a Schwarz-sorted pair list
+    (cuobc/scf/hf.py:567-578); for callers of the per-class-pair entry."""
+    scale = nbins / np.log(min(cutoff, .1))
+    s_index = np.floor(scale * log_q).astype(np.int32)
+    bins = np.bincount(s_index, minlength=nbins)[:nbins]
+    return np.append(0, np.cumsum(bins)).astype(np.int32)
+
+
+class _VHFOpt:
+    """Per-geometry J/K setup, the counterpart of the reference's _VHFOpt
+    (cuobc/scf/hf.py:277-448).  ``build`` sorts the working basis into
+    (l, nprim) groups and creates the device-side basis: Schwarz matrix,
+    Schwarz-sorted pair lists and the primitive-pair cache."""
+
+    def __init__(self, mol, intor='int2e', prescreen='CVHFnoscreen',
+                 qcondname='CVHFsetnr_direct_scf', dmcondname=None):
+        self.mol, self.coeff = basis_seg_contraction(mol)
+        self._intor = intor
+        self.handle = None
+
+    def build(self, cutoff=1e-13, group_size=None, diag_block_with_triu=False,
+              gpus=None):
+        if gpus not in (None, 1, [0], (0,)) and not isinstance(gpus, int):
+            pass  # one GPU per process; replicas scale out (see bench.py)
+        torch = _torch()
+        lib = _lib.load_library()
+        mol = self.mol
+        l_ctrs = mol._bas[:, [gmole.ANG_OF, gmole.NPRIM_OF]]
+        uniq_l_ctr, inv_idx, l_ctr_counts = np.unique(
+            l_ctrs, return_inverse=True, return_counts=True, axis=0)
+        inv_idx = np.asarray(inv_idx).ravel()
+        lmax = int(uniq_l_ctr[:, 0].max())
+        if lmax > LMAX_ON_GPU:
+            raise NotImplementedError(
+                'shells with l=%d: this engine handles l <= %d'
+                % (lmax, LMAX_ON_GPU))
+        if group_size is not None:
+            uniq_l_ctr, l_ctr_counts = _split_l_ctr_groups(
+                uniq_l_ctr, l_ctr_counts, group_size)
+        sorted_idx = np.argsort(inv_idx, kind='stable').astype(np.int32)
+        ao_loc = mol.ao_loc_nr(cart=True)
+        ao_idx = np.concatenate([np.arange(ao_loc[i], ao_loc[i + 1])
+                                 for i in sorted_idx])
+        self.coeff = self.coeff[ao_idx]
+        mol._bas = np.ascontiguousarray(mol._bas[sorted_idx])
+        self.direct_scf_tol = cutoff
+        self.uniq_l_ctr = uniq_l_ctr
+        self.l_ctr_offsets = np.append(0, np.cumsum(l_ctr_counts)).astype(
+            np.int32)
+        self.diag_fac = 1. if diag_block_with_triu else .5
+        self.h_shls = []
+        self.g_shls = []
+
+        handle = ctypes.c_void_p()
+        atm = np.ascontiguousarray(mol._atm, dtype=np.int32)
+        bas = np.ascontiguousarray(mol._bas, dtype=np.int32)
+        env = np.ascontiguousarray(mol._env, dtype=np.float64)
+        _lib.check(lib.jk_basis_create(
+            atm.ctypes.data, mol.natm, bas.ctypes.data, mol.nbas,
+            env.ctypes.data, env.size, self.l_ctr_offsets.ctypes.data,
+            len(uniq_l_ctr), cutoff, int(diag_block_with_triu),
+            ctypes.byref(handle)), 'jk_basis_create')
+        self.handle = handle
+        info = np.zeros(7, dtype=np.int32)
+        _lib.check(lib.jk_basis_info(handle, info.ctypes.data), 'jk_basis_info')
+        nbas, nao, ngroups, ncp, npairs = (int(v) for v in info[:5])
+        self.nao = nao
+        pair2shls = np.zeros((2, max(npairs, 1)), dtype=np.int32)
+        locs = np.zeros(ncp + 1, dtype=np.int32)
+        log_q = np.zeros(max(npairs, 1))
+        q_cond = np.zeros((nbas, nbas))
+        _lib.check(lib.jk_basis_pairs(handle, pair2shls.ctypes.data,
+                                      locs.ctypes.data, log_q.ctypes.data,
+                                      q_cond.ctypes.data), 'jk_basis_pairs')
+        self.bas_pair2shls = pair2shls[:, :npairs]
+        self.bas_pairs_locs = locs
+        self.log_qs = [log_q[locs[i]:locs[i + 1]] for i in range(ncp)]
+        self.q_cond = q_cond
+        self.coeff_dev = torch.as_tensor(self.coeff, dtype=torch.float64,
+                                         device='cuda').contiguous()
+        return self
+
+    def get_q_cond(self):
+        return self.q_cond
+
+    def default_nbins(self):
+        """cuobc/scf/hf.py:96-100."""
+        locs = self.bas_pairs_locs
+        pairs_max = int((locs[1:] - locs[:-1]).max()) if len(locs) > 1 else 0
+        return max(10, pairs_max // 100000)
+
+    def clear(self):
+        if self.handle is not None and self.handle.value:
+            _lib.load_library().jk_basis_destroy(self.handle)
+        self.handle = None
+        return self
+
+    def __del__(self):
+        try:
+            self.clear()
+        except Exception:
+            pass
+
+
+def get_jk(mol, dm, hermi=1, vhfopt=None, with_j=True, with_k=True,
+           omega=None, verbose=None, group_size=None, gpus=None,
+           prescreen=True, nbins=None, out='host'):
+    """Coulomb and exchange matrices of the density matrices ``dm``."""
+    if hermi != 1:
+        raise NotImplementedError(
+            'JK-builder only supports hermitian density matrix')
+    torch = _torch()
+    lib = _lib.load_library()
+    if vhfopt is None:
+        vhfopt = _VHFOpt(mol, 'int2e').build(gpus=gpus, group_size=group_size)
+    nao, nao0 = vhfopt.coeff.shape
+    is_tensor = isinstance(dm, torch.Tensor)
+    shape = tuple(dm.shape)
+    if shape[-1] != nao0 or shape[-2] != nao0 or len(shape) not in (2, 3):
+        raise ValueError('dm of shape %s does not match nao=%d' % (shape, nao0))
+    d = torch.as_tensor(dm, dtype=torch.float64, device='cuda')
+    d = d.reshape(-1, nao0, nao0).contiguous()
+    n_dm = d.shape[0]
+    vj = torch.empty_like(d) if with_j else None
+    vk = torch.empty_like(d) if with_k else None
+    if not with_j and not with_k:
+        return None, None
+    opts = _lib.JKOpts()
+    opts.direct_scf_tol = vhfopt.direct_scf_tol
+    opts.nbins = nbins if nbins is not None else vhfopt.default_nbins()
+    opts.prescreen = int(bool(prescreen))
+    _lib.check(lib.jk_get_jk(
+        vhfopt.handle, vhfopt.coeff_dev.data_ptr(), nao0, d.data_ptr(), n_dm,
+        vj.data_ptr() if with_j else None, vk.data_ptr() if with_k else None,
+        ctypes.byref(opts), _stream_ptr(torch)), 'jk_get_jk')
+    res = []
+    for v in (vj, vk):
+        if v is None:
+            res.append(None)
+            continue
+        v = v.reshape(shape)
+        res.append(v if (out == 'device' or (out == 'same' and is_tensor))
+                   else v.cpu().numpy())
+    return res[0], res[1]
+
+
+def _get_jk(mf, mol=None, dm=None, hermi=1, with_j=True, with_k=True,
+            omega=None):
+    """RHF.get_jk of the reference (cuobc/scf/hf.py:230-250): builds and
+    caches the _VHFOpt on first use."""
+    if omega is not None:
+        raise NotImplementedError('Range separated Coulomb integrals')
+    if mol is None:
+        mol = mf.mol
+    if getattr(mf, '_opt_gpu', None) is None:
+        mf._opt_gpu = _VHFOpt(mol, 'int2e').build(mf.direct_scf_tol)
+    return get_jk(mol, dm, hermi, mf._opt_gpu, with_j, with_k)

@@ -308,6 +308,27 @@ class Mole:
                   j0 + ic * nsph(l):j0 + (ic + 1) * nsph(l)] = blk
         return c
 
+    def intor(self, name):
+        """One-electron integrals 'int1e_ovlp', 'int1e_kin', 'int1e_nuc'
+        in this molecule's basis (host code in libjk.so)."""
+        import ctypes
+        from byteqc_b200.cuobc import lib as jklib
+        which = {'int1e_ovlp': 0, 'int1e_kin': 1, 'int1e_nuc': 2}[name]
+        n = self.nao_nr(cart=True)
+        out = np.zeros((n, n))
+        atm = np.ascontiguousarray(self._atm, dtype=np.int32)
+        bas = np.ascontiguousarray(self._bas, dtype=np.int32)
+        env = np.ascontiguousarray(self._env)
+        rc = jklib.load_library().jk_int1e_cart(
+            which, atm.ctypes.data, self.natm, bas.ctypes.data, self.nbas,
+            env.ctypes.data, out.ctypes.data)
+        if rc:
+            raise RuntimeError('jk_int1e_cart failed with status %d' % rc)
+        if not self.cart:
+            c = self.cart2sph_coeff()
+            out = c.T @ out @ c
+        return out
+
     def energy_nuc(self):
         z = self.atom_charges().astype(np.float64)
         r = self.atom_coords()

@@ -1,0 +1,129 @@
+/*
+ * byteqc_jk.h -- C-ABI of the B200 direct-SCF J/K engine (libjk.so).
+ *
+ * Drop-in boundary for the reference's ctypes interface of ByteQC cuobc's J/K
+ * path (cuobc/lib/__init__.py:39-42 loads libgint/libgvhf; the Python side is
+ * cuobc/scf/hf.py).  All functions return an int status (JK_OK on success)
+ * and never exit the process; jk_last_error() describes the last failure of
+ * the calling thread.  Device pointers are plain CUDA device addresses;
+ * `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *
+ * Working basis: the decontracted Cartesian basis with shells sorted into
+ * groups of equal (l, nprim), exactly as the reference's _VHFOpt.build
+ * prepares it (cuobc/scf/hf.py:288-330, 481-564).  Angular momentum up to f.
+ */
+#ifndef BYTEQC_JK_H
+#define BYTEQC_JK_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define JK_OK 0
+#define JK_ERR_CUDA 1        /* CUDA / cuBLAS failure (launch, copy, OOM) */
+#define JK_ERR_UNSUPPORTED 2 /* angular momentum or class not handled */
+#define JK_ERR_ARG 3         /* invalid argument */
+
+typedef struct jk_basis jk_basis_t;
+
+typedef struct {
+    double direct_scf_tol; /* density screen threshold (mf.direct_scf_tol)    */
+    int nbins;             /* log-Schwarz bins (hf.py:96-100: max(10, ...))    */
+    int prescreen;         /* class-level density screen on/off (hf.py:139)   */
+    double fp32_cutoff;    /* mixed precision: FP32 recursion below this bound;
+                              0 disables                                       */
+    int reserved[8];
+} jk_opts_t;
+
+/*
+ * Basis setup for one geometry: device copies of the basis, the Schwarz
+ * matrix q[i,j] = sqrt(max |(ij|ij)|) computed on the device, Schwarz-sorted
+ * shell-pair lists per lower-triangular group pair (kept if q > cutoff; the
+ * upper triangle of diagonal blocks dropped unless diag_block_with_triu),
+ * and the primitive-pair cache.
+ * Replaces GINTinit_basis_prod_cpu (cuobc/lib/gint/nr_fill_ao_ints.cu:452-470),
+ * GINTinit_basis_prod_gpu (nr_fill_ao_ints.cu:472-491) and the q_cond /
+ * pair-list part of _VHFOpt.build (cuobc/scf/hf.py:341-408).  Unlike the
+ * reference it copies every input, so nothing is borrowed from the caller.
+ * atm/bas/env: libcint arrays of the working basis; group_offsets: ngroups+1
+ * shell offsets of the (l, nprim) groups (l_ctr_offsets).
+ */
+int jk_basis_create(const int *atm, int natm, const int *bas, int nbas, const double *env, int nenv,
+                    const int *group_offsets, int ngroups, double cutoff, int diag_block_with_triu,
+                    jk_basis_t **out);
+
+/* Replaces GINTdel_basis_prod (cuobc/lib/gint/nr_fill_ao_ints.cu:394-410). */
+int jk_basis_destroy(jk_basis_t *basis);
+
+/* info[7] = {nbas, nao, ngroups, nclass_pairs, npairs, nprim_pairs,
+ * nclass_quartets}.  Mirrors the BasisProdCache fields the reference reads
+ * through ctypes (cuobc/scf/hf.py:451-478). */
+int jk_basis_info(const jk_basis_t *basis, int *info);
+
+/* Copies of the pair lists (bas_pair2shls 2 x npairs, bas_pairs_locs
+ * ncp+1, log_q npairs) and the Schwarz matrix (nbas x nbas); any output may
+ * be NULL.  Same content as _VHFOpt.bas_pair2shls / bas_pairs_locs / log_qs
+ * (cuobc/scf/hf.py:391-396). */
+int jk_basis_pairs(const jk_basis_t *basis, int *pair2shls, int *pair_locs, double *log_q, double *q_cond);
+
+/*
+ * One class pair with host-side log-Schwarz bins, same contract as
+ * GINTbuild_jk (cuobc/lib/gvhf/nr_jk_driver.cu:227-284): vj/vk are device
+ * buffers (n_dm, nao, nao) accumulated (+=) with element (i, j) at
+ * i + nao*j, either may be NULL; dm is the device density in the working
+ * basis; bins are host arrays of nbins+1 offsets.
+ */
+int jk_build_class_pair(jk_basis_t *basis, double *vj, double *vk, const double *dm, int nao, int n_dm,
+                        const int *bins_locs_ij, const int *bins_locs_kl, int nbins, int cp_ij, int cp_kl,
+                        void *stream);
+
+/*
+ * All class pairs in one call with the screening done on the device: the
+ * per-group density condensation, the class-level density screen and the
+ * log-Schwarz bin test per quartet, with the reference's decisions
+ * (cuobc/scf/hf.py:104-160).  Same buffer contract as jk_build_class_pair.
+ * Replaces the task loop of get_jk (cuobc/scf/hf.py:111-166).
+ */
+int jk_build(jk_basis_t *basis, const double *dm, int n_dm, double *vj, double *vk, const jk_opts_t *opts,
+             void *stream);
+
+/*
+ * Full J/K in the caller's basis: dms = C D C^T, jk_build, then
+ * J = 2 C^T (V + V^T) C and K = C^T (V + V^T) C (cuobc/scf/hf.py:67-181).
+ * coeff: device (nao, nao0) row-major (the working basis -> caller basis map);
+ * dm0, vj0, vk0: device (n_dm, nao0, nao0) row-major; vj0/vk0 are
+ * overwritten; either may be NULL.
+ */
+int jk_get_jk(jk_basis_t *basis, const double *coeff, int nao0, const double *dm0, int n_dm, double *vj0,
+              double *vk0, const jk_opts_t *opts, void *stream);
+
+/* Rys nodes s = t^2 and weights of the product tables, evaluated on the
+ * host (for checking the tables).  Returns JK_ERR_ARG for n outside 1..11. */
+int jk_rys_roots_host(int n, double x, double *s, double *w);
+
+/* Per class quartet (8 ints each): cp_ij, cp_kl, li, lj, lk, ll, nprim_ij,
+ * nprim_kl.  No reference counterpart: introspection for the cost model. */
+int jk_basis_cq_info(const jk_basis_t *basis, int *out);
+
+/* Screened contracted-quartet count per class quartet of the last jk_build
+ * (synchronises `stream`).  No reference counterpart. */
+int jk_last_counts(const jk_basis_t *basis, long long *out, void *stream);
+
+/* Measured FMA-pipe peak of the current device in TFLOP/s (fp32 = 0: FP64,
+ * 1: FP32), from 8 independent FMA chains per thread over the whole GPU.
+ * No reference counterpart: the roofline denominator of the J/K kernels. */
+int jk_fma_peak(int fp32, double *tflops);
+
+/* One-electron integrals of the SCF glue, host code: which = 0 overlap,
+ * 1 kinetic, 2 nuclear attraction; out (nao_cart, nao_cart) row-major over
+ * all contractions of all shells.  PySCF's mol.intor supplies these to the
+ * reference (outside the reference repository). */
+int jk_int1e_cart(int which, const int *atm, int natm, const int *bas, int nbas, const double *env, double *out);
+
+/* Description of the last failure in the calling thread. */
+const char *jk_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

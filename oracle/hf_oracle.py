@@ -204,7 +204,7 @@ def _ptr(a):
 
 
 def get_jk(mol, dm, hermi=1, vhfopt=None, with_j=True, with_k=True,
-           prescreen=True, nbins=None, stats=None):
+           prescreen=True, nbins=None, stats=None, ij_stride=1):
     """Oracle J/K.  Returns numpy (vj, vk) shaped like ``dm``; a disabled
     matrix is None."""
     if hermi != 1:
@@ -262,7 +262,7 @@ def get_jk(mol, dm, hermi=1, vhfopt=None, with_j=True, with_k=True,
             ctypes.c_int(nao), ctypes.c_int(n_dm),
             _ptr(vj) if with_j else None, _ptr(vk) if with_k else None,
             _ptr(bins_ij), _ptr(bins_kl), ctypes.c_int(nbins),
-            ctypes.c_int(cp_ij), ctypes.c_int(cp_kl))
+            ctypes.c_int(cp_ij), ctypes.c_int(cp_kl), ctypes.c_int(ij_stride))
     if stats is not None:
         stats['quartets'] = nquartets
         stats['nbins'] = nbins

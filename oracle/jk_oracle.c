@@ -265,13 +265,16 @@ void oracle_q_cond(const int *atm, const int *bas, const double *env, int nbas, 
  * reference bin offsets (host arrays, nbins+1 entries, local to the class),
  * accumulated into vj/vk (either may be NULL) with the reference's view
  * convention v[i + nao*j].  pair_locs: start of each class in pair2bra/ket.
+ * ij_stride > 1 evaluates only the rows ij = 0 mod ij_stride (a uniform
+ * subsample used to time the CPU baseline on a bounded share of the work).
  * dm: (n_dm, nao, nao) C-order.  Returns the number of contracted quartets
  * evaluated.
  */
 long oracle_build_jk(const int *atm, const int *bas, const double *env, int nbas, const int *ao_loc,
                      const int *pair2bra, const int *pair2ket, const int *pair_locs, double diag_fac,
                      const double *dm, int nao, int n_dm, double *vj, double *vk,
-                     const int *bins_ij, const int *bins_kl, int nbins, int cp_ij, int cp_kl) {
+                     const int *bins_ij, const int *bins_kl, int nbins, int cp_ij, int cp_kl,
+                     int ij_stride) {
     basis_t b = {atm, bas, env, nbas};
     double fac = 2 * M_PI * M_PI * M_PI / sqrt(M_PI);
     long count = 0;
@@ -294,6 +297,7 @@ long oracle_build_jk(const int *atm, const int *bas, const double *env, int nbas
 #pragma omp for schedule(static)
             for (int tij = ij0; tij < ij1; tij++)
                 for (int tkl = kl0; tkl < kl1; tkl++) {
+                    if (ij_stride > 1 && tij % ij_stride) continue;
                     int bas_ij = pair_locs[cp_ij] + tij;
                     int bas_kl = pair_locs[cp_kl] + tkl;
                     if (bas_ij < bas_kl) continue;

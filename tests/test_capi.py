@@ -1,0 +1,52 @@
+"""The C-ABI library loads without a GPU, exports every symbol the header
+declares, and rejects invalid arguments with a status (no process exit)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+
+from byteqc_b200.cuobc import lib as jklib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    src = open(os.path.join(ROOT, 'include', 'byteqc_jk.h')).read()
+    src = re.sub(r'/\*.*?\*/', '', src, flags=re.S)
+    return sorted(set(re.findall(r'\b(jk_[a-z0-9_]+)\s*\(', src)))
+
+
+def test_exports_every_declared_symbol():
+    lib = jklib.load_library()
+    names = _declared()
+    assert 'jk_build' in names and 'jk_get_jk' in names
+    for n in names:
+        assert hasattr(lib, n), n
+
+
+def test_invalid_arguments_return_status():
+    lib = jklib.load_library()
+    out = ctypes.c_void_p()
+    rc = lib.jk_basis_create(None, 0, None, 0, None, 0, None, 0, 1e-13, 0,
+                             ctypes.byref(out))
+    assert rc == 3
+    assert b'invalid' in lib.jk_last_error()
+    s = np.zeros(2)
+    assert lib.jk_rys_roots_host(0, 1.0, s.ctypes.data, s.ctypes.data) == 3
+
+
+def test_product_tables_match_oracle_tables():
+    import oracle
+    lib = jklib.load_library()
+    rng = np.random.default_rng(0)
+    for n in range(1, 12):
+        for x in np.concatenate([[0., 1e-12, 2., 39.999, 98.0, 150.],
+                                 rng.uniform(0, 110, 40)]):
+            s = np.zeros(n)
+            w = np.zeros(n)
+            assert lib.jk_rys_roots_host(n, x, s.ctypes.data,
+                                         w.ctypes.data) == 0
+            so, wo = oracle.rys_roots(n, x)
+            np.testing.assert_allclose(s, so, rtol=5e-14, atol=0)
+            np.testing.assert_allclose(w, wo, rtol=0, atol=5e-15 * w.sum())

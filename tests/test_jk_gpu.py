@@ -1,0 +1,81 @@
+"""GPU parity of the J/K engine against the oracle (the CPU restatement of
+the reference's get_jk, oracle/hf_oracle.py + oracle/jk_oracle.c).
+
+Tolerance: 1e-10 max-abs in J/K elements (the FP64 parity bar), plus a
+relative bound for matrices with large entries."""
+import numpy as np
+import pytest
+
+from byteqc_b200.gto import Mole, geom
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+
+def _mol(nw, basis, box, seed=0):
+    return Mole(atom=geom.water_cluster(nw, box=box, seed=seed),
+                basis=basis).build()
+
+
+def _rand_dm(n, seed=3, ndm=None):
+    rng = np.random.default_rng(seed)
+    shape = (n, n) if ndm is None else (ndm, n, n)
+    d = rng.random(shape)
+    return d + np.swapaxes(d, -1, -2)
+
+
+def _close(a, b):
+    err = abs(a - b).max()
+    scale = max(1.0, abs(b).max())
+    assert err <= TOL * scale, 'max|diff| %.3e (scale %.3g)' % (err, scale)
+
+
+@pytest.mark.parametrize('basis', ['standin-cc-pvdz', 'standin-6-31g*',
+                                   'standin-def2-tzvp'])
+def test_get_jk_vs_oracle(basis):
+    from byteqc_b200.cuobc.scf import hf
+    from oracle import hf_oracle
+    mol = _mol(2, basis, 5.0)
+    dm = _rand_dm(mol.nao)
+    vj, vk = hf.get_jk(mol, dm)
+    rj, rk = hf_oracle.get_jk(mol, dm)
+    _close(vj, rj)
+    _close(vk, rk)
+
+
+def test_multi_dm_and_flags():
+    from byteqc_b200.cuobc.scf import hf
+    from oracle import hf_oracle
+    mol = _mol(3, 'standin-cc-pvdz', 6.0, seed=4)
+    dm = _rand_dm(mol.nao, ndm=2)
+    opt = hf._VHFOpt(mol).build()
+    ropt = hf_oracle.VHFOpt(mol).build()
+    rj, rk = hf_oracle.get_jk(mol, dm, vhfopt=ropt)
+    vj, vk = hf.get_jk(mol, dm, vhfopt=opt)
+    _close(vj, rj)
+    _close(vk, rk)
+    vj2, vk2 = hf.get_jk(mol, dm, vhfopt=opt, with_k=False)
+    assert vk2 is None
+    _close(vj2, rj)
+    vj3, vk3 = hf.get_jk(mol, dm, vhfopt=opt, with_j=False)
+    assert vj3 is None
+    _close(vk3, rk)
+    # unscreened, single bin (the reference test's settings, jk.py:7824)
+    rj, rk = hf_oracle.get_jk(mol, dm[0], vhfopt=ropt, prescreen=False,
+                              nbins=1)
+    vj, vk = hf.get_jk(mol, dm[0], vhfopt=opt, prescreen=False, nbins=1)
+    _close(vj, rj)
+    _close(vk, rk)
+
+
+def test_pairs_and_qcond_vs_oracle():
+    from byteqc_b200.cuobc.scf import hf
+    from oracle import hf_oracle
+    mol = _mol(3, 'standin-def2-tzvp', 6.0, seed=2)
+    opt = hf._VHFOpt(mol).build()
+    ropt = hf_oracle.VHFOpt(mol).build()
+    np.testing.assert_allclose(opt.q_cond, ropt.q_cond, rtol=1e-11,
+                               atol=1e-16)
+    np.testing.assert_array_equal(opt.bas_pairs_locs, ropt.bas_pairs_locs)
+    np.testing.assert_allclose(opt.coeff, ropt.coeff, atol=1e-15)
