@@ -281,8 +281,8 @@ def main():
     counts = np.zeros(max(ncq, 1), dtype=np.int64)
     lib.jk_last_counts(opt.handle, counts.ctypes.data, sptr)
     quartets = int(counts[:ncq].sum())
-    flops = sum(int(c) * class_flops(*cq[i, 2:8]) for i, c in
-                enumerate(counts[:ncq]) if c)
+    flops = sum(int(c) * class_flops(*(int(v) for v in cq[i, 2:8]))
+                for i, c in enumerate(counts[:ncq]) if c)
     peak = ctypes.c_double()
     lib.jk_fma_peak(0, ctypes.byref(peak))
     achieved = flops / (ms_kern * 1e-3) / 1e12
@@ -310,7 +310,8 @@ def main():
         'quartets_per_s': world * quartets / (ms_step * 1e-3),
         'kernel_ms_per_build': ms_kern,
         'setup_s': setup_s,
-        'gpu_launches': 2 + int((counts[:ncq] >= 0).sum()) + 2,
+        # dm_cond + screen + one launch per class quartet + 2 symmetrize
+        'gpu_launches': 4 + ncq,
         'roofline': {'bound': 'fp64', 'achieved': achieved,
                      'peak': peak.value, 'unit': 'TFLOP/s',
                      'frac': achieved / peak.value if peak.value else None,
@@ -330,7 +331,7 @@ def main():
             'sample': 'oracle J/K on every %d-th shell-pair row of each class '
                       'pair (%.1f s of CPU work), scaled to one build'
                       % (inf['stride'], inf['sample_s'])}
-    print(json.dumps(line))
+    print(json.dumps(line, default=float))
     if dist:
         dist.destroy_process_group()
 

@@ -5,12 +5,18 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#ifndef RYS_STORAGE
-#define RYS_STORAGE __device__ const
-#endif
+// The small per-n metadata is in constant memory of every module; the
+// Chebyshev coefficients (about 0.6 MB) are uploaded once per device into
+// global memory and reached through a pointer (JKSeg::rys), read with __ldg.
+#define RYS_META static __constant__
 #include "rys_table.h"
 
 #define JK_LMAX 3  // angular momentum handled by the templated kernels
+
+// 2 pi^3 / sqrt(pi): prefactor of the two-electron integrals (the seed of the
+// x 2D integrals; cuobc/lib/gint/g2e.c:41)
+#define JK_FAC (2.0 * 3.14159265358979323846 * 3.14159265358979323846 * 3.14159265358979323846 / \
+                1.77245385090551602730)
 
 // ---------------------------------------------------------------------------
 // Rys nodes s_r = t_r^2 and weights w_r at x = rho |P-Q|^2 from the generated
@@ -30,7 +36,8 @@ __device__ __forceinline__ double rys_cheb(const double* __restrict__ c, double 
 }
 
 template <int N>
-__device__ __forceinline__ void rys_root(double x, int r, double& s, double& w) {
+__device__ __forceinline__ void rys_root(const double* __restrict__ rys_coef, double x, int r, double& s,
+                                         double& w) {
     if (x >= rys_xmax[N]) {
         int b = N * (N - 1) / 2 + r;
         double rx = 1. / x;
@@ -159,6 +166,7 @@ __device__ __forceinline__ void rys_2d(R seed, R c00, R c0p, R b10, R b01, R b00
 // row ij holds kl = 0 .. nkl(ij)-1 and qoff is the exclusive prefix of nkl.
 // ---------------------------------------------------------------------------
 struct JKSeg {
+    const double* rys;      // Rys coefficient table (device)
     const long long* qoff;  // n_ij + 1 entries (device)
     int n_ij;
     int pair_ij0, pair_kl0;  // first pair of each class in the pair arrays

@@ -46,11 +46,7 @@ static jk_launch_fn g_tab64[256], g_tab32[256];
 static std::once_flag g_tab_once;
 static void init_tables() {
     std::call_once(g_tab_once, [] {
-        jk_register_l0(g_tab64, g_tab32);
-        jk_register_l1(g_tab64, g_tab32);
-        jk_register_l2(g_tab64, g_tab32);
-        jk_register_l3a(g_tab64, g_tab32);
-        jk_register_l3b(g_tab64, g_tab32);
+        JK_REGISTER_ALL();
     });
 }
 
@@ -78,7 +74,8 @@ static double common_fac_sp(int l) {
 template <int LI, int LJ>
 __global__ void jk_qcond_kernel(const int* __restrict__ pi, const int* __restrict__ pj, int npairs,
                                 const int* __restrict__ atm, const int* __restrict__ bas,
-                                const double* __restrict__ env, int nbas, double* __restrict__ q) {
+                                const double* __restrict__ env, int nbas, double* __restrict__ q,
+                                const double* __restrict__ rys) {
     using C = JKClass<LI, LJ, LI, LJ>;
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= npairs) return;
@@ -121,11 +118,11 @@ __global__ void jk_qcond_kernel(const int* __restrict__ pi, const int* __restric
                     pr.sy = eij * ekl / (sqrt(pr.AB) * A * B);
                     for (int r = 0; r < C::NROOTS; r++) {
                         double s, w;
-                        rys_root<C::NROOTS>(pr.x, r, s, w);
+                        rys_root<C::NROOTS>(rys, pr.x, r, s, w);
                         double Ix[C::GS], Iy[C::GS], Iz[C::GS];
-                        jk_unit<C, double>(pr, s, w, 0, 11.13665599366341569, r_i, r_j, r_i, r_j, Ix);
-                        jk_unit<C, double>(pr, s, w, 1, 11.13665599366341569, r_i, r_j, r_i, r_j, Iy);
-                        jk_unit<C, double>(pr, s, w, 2, 11.13665599366341569, r_i, r_j, r_i, r_j, Iz);
+                        jk_unit<C, double>(pr, s, w, 0, JK_FAC, r_i, r_j, r_i, r_j, Ix);
+                        jk_unit<C, double>(pr, s, w, 1, JK_FAC, r_i, r_j, r_i, r_j, Iy);
+                        jk_unit<C, double>(pr, s, w, 2, JK_FAC, r_i, r_j, r_i, r_j, Iz);
 #pragma unroll
                         for (int a = 0; a < C::NFI; a++)
 #pragma unroll
@@ -147,11 +144,11 @@ __global__ void jk_qcond_kernel(const int* __restrict__ pi, const int* __restric
 }
 
 typedef void (*qcond_fn)(const int*, const int*, int, const int*, const int*, const double*, int, double*,
-                         cudaStream_t);
+                         const double*, cudaStream_t);
 template <int LI, int LJ>
 static void qcond_launch(const int* pi, const int* pj, int n, const int* atm, const int* bas, const double* env,
-                         int nbas, double* q, cudaStream_t st) {
-    if (n > 0) jk_qcond_kernel<LI, LJ><<<(n + 63) / 64, 64, 0, st>>>(pi, pj, n, atm, bas, env, nbas, q);
+                         int nbas, double* q, const double* rys, cudaStream_t st) {
+    if (n > 0) jk_qcond_kernel<LI, LJ><<<(n + 63) / 64, 64, 0, st>>>(pi, pj, n, atm, bas, env, nbas, q, rys);
 }
 static qcond_fn g_qcond[4][4] = {
     {qcond_launch<0, 0>, nullptr, nullptr, nullptr},
@@ -292,6 +289,7 @@ __global__ void jk_symmetrize_kernel(const double* __restrict__ in, double* __re
 // ---------------------------------------------------------------------------
 struct jk_basis {
     int device = 0, nsm = 148;
+    const double* rys = nullptr;  // shared per-device Rys table
     int natm = 0, nbas = 0, nao = 0, ngroups = 0, ncp = 0, ncq = 0;
     double diag_fac = 0.5, cutoff = 1e-13;
     std::vector<int> h_ao_loc, h_group_off, h_group_l, h_group_nprim;
@@ -363,11 +361,40 @@ static cudaError_t upload(T** dst, const T* src, size_t n) {
 }
 
 extern "C" int jk_rys_table_uniform(void);
+extern "C" const double* jk_rys_coef_host(long long* count);
+
+// Rys coefficient table in global memory, one copy per device, kept until exit
+static std::mutex g_rys_mu;
+static double* g_rys_dev[64];
+static int rys_table_device(const double** out) {
+    int dev;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return set_err(JK_ERR_ARG, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lk(g_rys_mu);
+    if (!g_rys_dev[dev]) {
+        long long n;
+        const double* h = jk_rys_coef_host(&n);
+        double* d;
+        CUDA_TRY(cudaMalloc(&d, sizeof(double) * n));
+        cudaError_t e = cudaMemcpy(d, h, sizeof(double) * n, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            cudaFree(d);
+            CUDA_TRY(e);
+        }
+        g_rys_dev[dev] = d;
+    }
+    *out = g_rys_dev[dev];
+    return JK_OK;
+}
 
 static int create_impl(const int* atm, int natm, const int* bas, int nbas, const double* env, int nenv,
                        const int* group_off, int ngroups, double cutoff, int diag_block_with_triu, jk_basis* b) {
     init_tables();
     if (!jk_rys_table_uniform()) return set_err(JK_ERR_ARG, "Rys tables must use intervals of width 2");
+    {
+        int rc = rys_table_device(&b->rys);
+        if (rc) return rc;
+    }
     CUDA_TRY(cudaGetDevice(&b->device));
     CUDA_TRY(cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, b->device));
     b->natm = natm;
@@ -436,7 +463,7 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
                 int *dpi, *dpj;
                 CUDA_TRY(upload(&dpi, pi[a][c].data(), n));
                 CUDA_TRY(upload(&dpj, pj[a][c].data(), n));
-                g_qcond[a][c](dpi, dpj, n, b->d_atm, b->d_bas, b->d_env, nbas, b->d_qcond, 0);
+                g_qcond[a][c](dpi, dpj, n, b->d_atm, b->d_bas, b->d_env, nbas, b->d_qcond, b->rys, 0);
                 cudaError_t e = cudaGetLastError();
                 if (e == cudaSuccess) e = cudaDeviceSynchronize();
                 cudaFree(dpi);
@@ -600,6 +627,7 @@ extern "C" int jk_basis_pairs(const jk_basis_t* b, int* pair2shls, int* pair_loc
 
 static void fill_seg(const jk_basis* b, int cp_ij, int cp_kl, const long long* qoff, int n_ij, const double* dm,
                      int n_dm, double* vj, double* vk, JKSeg* s) {
+    s->rys = b->rys;
     s->qoff = qoff;
     s->n_ij = n_ij;
     s->pair_ij0 = b->h_pair_locs[cp_ij];
@@ -855,5 +883,39 @@ extern "C" int jk_fma_peak(int fp32, double* tflops) {
     cudaEventDestroy(e1);
     cudaFree(buf);
     *tflops = best;
+    return JK_OK;
+}
+
+// device evaluation of the Rys tables at a batch of points (checks the
+// device copy of the tables against the host evaluation)
+template <int N>
+__global__ void jk_rys_eval_kernel(const double* rys, const double* x, int count, double* s, double* w) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    for (int r = 0; r < N; r++) rys_root<N>(rys, x[i], r, s[i * N + r], w[i * N + r]);
+}
+
+extern "C" int jk_rys_roots_device(int n, const double* x, int count, double* s, double* w, void* stream) {
+    if (n < 1 || n > 11 || !x || !s || !w || count < 0) return set_err(JK_ERR_ARG, "jk_rys_roots_device: bad args");
+    if (count == 0) return JK_OK;
+    const double* rys;
+    int rc = rys_table_device(&rys);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    int nb = (count + 127) / 128;
+    switch (n) {
+        case 1: jk_rys_eval_kernel<1><<<nb, 128, 0, st>>>(rys, x, count, s, w); break;
+        case 2: jk_rys_eval_kernel<2><<<nb, 128, 0, st>>>(rys, x, count, s, w); break;
+        case 3: jk_rys_eval_kernel<3><<<nb, 128, 0, st>>>(rys, x, count, s, w); break;
+        case 4: jk_rys_eval_kernel<4><<<nb, 128, 0, st>>>(rys, x, count, s, w); break;
+        case 5: jk_rys_eval_kernel<5><<<nb, 128, 0, st>>>(rys, x, count, s, w); break;
+        case 6: jk_rys_eval_kernel<6><<<nb, 128, 0, st>>>(rys, x, count, s, w); break;
+        case 7: jk_rys_eval_kernel<7><<<nb, 128, 0, st>>>(rys, x, count, s, w); break;
+        case 8: jk_rys_eval_kernel<8><<<nb, 128, 0, st>>>(rys, x, count, s, w); break;
+        case 9: jk_rys_eval_kernel<9><<<nb, 128, 0, st>>>(rys, x, count, s, w); break;
+        case 10: jk_rys_eval_kernel<10><<<nb, 128, 0, st>>>(rys, x, count, s, w); break;
+        default: jk_rys_eval_kernel<11><<<nb, 128, 0, st>>>(rys, x, count, s, w); break;
+    }
+    CUDA_TRY(cudaGetLastError());
     return JK_OK;
 }

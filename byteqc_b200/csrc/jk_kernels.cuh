@@ -60,7 +60,7 @@ __device__ __forceinline__ JKQuartet jk_decode(const JKSeg& sg, long long local)
     q.prim_ij = sg.prim_ij0 + row * sg.nprim_ij;
     q.prim_kl = sg.prim_kl0 + col * sg.nprim_kl;
     // 2 pi^3 / sqrt(pi), halved on the ij == kl diagonal (g2e.c:41, g2e.cu:1025)
-    q.norm = 11.13665599366341569 * (bij == bkl ? 0.5 : 1.0);
+    q.norm = JK_FAC * (bij == bkl ? 0.5 : 1.0);
     return q;
 }
 
@@ -137,7 +137,7 @@ __device__ __forceinline__ void jk_thread_quartet(const JKSeg& sg, const JKQuart
 #pragma unroll
             for (int r = 0; r < NR; r++) {
                 double s, w;
-                rys_root<NR>(p.x, r, s, w);
+                rys_root<NR>(sg.rys, p.x, r, s, w);
                 R Ix[C::GS], Iy[C::GS], Iz[C::GS];
                 jk_unit<C, R>(p, s, w, 0, q.norm, ri, rj, rk, rl, Ix);
                 jk_unit<C, R>(p, s, w, 1, q.norm, ri, rj, rk, rl, Iy);
@@ -327,7 +327,7 @@ __global__ void jk_team_kernel(const JKSeg* __restrict__ segs, const long long* 
                     for (int u = lane; u < 3 * NR; u += T) {
                         int r = u / 3, d = u - 3 * r;
                         double s, w;
-                        rys_root<NR>(p.x, r, s, w);
+                        rys_root<NR>(sg.rys, p.x, r, s, w);
                         jk_unit<C, R>(p, s, w, d, q.norm, ri, rj, rk, rl, g + u * C::GS);
                     }
                 }

@@ -34,13 +34,14 @@ cudaError_t jk_launch(const JKSeg* segs, const long long* task0, int nseg, long 
     return cudaGetLastError();
 }
 
-// per-instantiation-file registration
-void jk_register_l0(jk_launch_fn* tab64, jk_launch_fn* tab32);
-void jk_register_l1(jk_launch_fn* tab64, jk_launch_fn* tab32);
-void jk_register_l2(jk_launch_fn* tab64, jk_launch_fn* tab32);
-void jk_register_l3a(jk_launch_fn* tab64, jk_launch_fn* tab32);
-void jk_register_l3b(jk_launch_fn* tab64, jk_launch_fn* tab32);
+// per-instantiation-file registration (jk_inst_*.cu, generated list)
+#include "jk_inst_list.h"
 
+#ifdef JK_WITH_FP32
+#define JK_REG32(LI, LJ, LK, LL) tab32[(LI)*64 + (LJ)*16 + (LK)*4 + (LL)] = jk_launch<LI, LJ, LK, LL, float>;
+#else
+#define JK_REG32(LI, LJ, LK, LL)
+#endif
 #define JK_REG(LI, LJ, LK, LL)                                                     \
     tab64[(LI)*64 + (LJ)*16 + (LK)*4 + (LL)] = jk_launch<LI, LJ, LK, LL, double>; \
-    tab32[(LI)*64 + (LJ)*16 + (LK)*4 + (LL)] = jk_launch<LI, LJ, LK, LL, float>;
+    JK_REG32(LI, LJ, LK, LL)

@@ -2,7 +2,8 @@
 // device evaluates in jk_common.cuh), exported for checking the tables.
 #include <math.h>
 
-#define RYS_STORAGE static const
+#define RYS_META static const
+#define RYS_WANT_COEF
 #include "rys_table.h"
 
 #include "../../include/byteqc_jk.h"
@@ -43,4 +44,10 @@ extern "C" int jk_rys_table_uniform(void) {
     for (int n = 1; n <= RYS_NMAX; n++)
         if (rys_h[n] != 2.0) return 0;
     return 1;
+}
+
+// the coefficient table, uploaded to each device by the engine
+extern "C" const double* jk_rys_coef_host(long long* count) {
+    if (count) *count = RYS_TOTAL;
+    return rys_coef;
 }

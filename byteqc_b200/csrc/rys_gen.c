@@ -233,30 +233,33 @@ int main(int argc, char **argv) {
         off[n + 1] = off[n] + nint[n] * 2 * n * NC;
     }
     fprintf(fo, "/* generated by rys_gen.c: Rys nodes s=t^2 and weights, %d-term Chebyshev\n"
-                " * series on uniform intervals, Gauss-Hermite limit beyond. */\n", NC);
+                " * series on uniform intervals, Gauss-Hermite limit beyond.  The small\n"
+                " * metadata arrays use RYS_META storage; the coefficient array is emitted\n"
+                " * only where RYS_WANT_COEF is defined (one host translation unit). */\n", NC);
     fprintf(fo, "#define RYS_NC %d\n#define RYS_NMAX %d\n#define RYS_TOTAL %d\n", NC, nmax, off[nmax + 1]);
-    fprintf(fo, "RYS_STORAGE double rys_h[%d] = {0", nmax + 1);
+    fprintf(fo, "#ifndef RYS_META\n#define RYS_META static const\n#endif\n");
+    fprintf(fo, "RYS_META double rys_h[%d] = {0", nmax + 1);
     for (int n = 1; n <= nmax; n++) fprintf(fo, ", %a", hs[n]);
-    fprintf(fo, "};\nRYS_STORAGE double rys_xmax[%d] = {0", nmax + 1);
+    fprintf(fo, "};\nRYS_META double rys_xmax[%d] = {0", nmax + 1);
     for (int n = 1; n <= nmax; n++) fprintf(fo, ", %a", xas[n]);
-    fprintf(fo, "};\nRYS_STORAGE int rys_nint[%d] = {0", nmax + 1);
+    fprintf(fo, "};\nRYS_META int rys_nint[%d] = {0", nmax + 1);
     for (int n = 1; n <= nmax; n++) fprintf(fo, ", %d", nint[n]);
-    fprintf(fo, "};\nRYS_STORAGE int rys_off[%d] = {0", nmax + 1);
+    fprintf(fo, "};\nRYS_META int rys_off[%d] = {0", nmax + 1);
     for (int n = 1; n <= nmax; n++) fprintf(fo, ", %d", off[n]);
     fprintf(fo, "};\n/* Gauss-Hermite limit, node-major: index n*(n-1)/2 + i */\n");
-    fprintf(fo, "RYS_STORAGE double rys_herm_r[%d] = {", nmax * (nmax + 1) / 2);
+    fprintf(fo, "RYS_META double rys_herm_r[%d] = {", nmax * (nmax + 1) / 2);
     for (int n = 1; n <= nmax; n++)
         for (int i = 0; i < n; i++) fprintf(fo, "%s%a", (n == 1 && i == 0) ? "" : ", ", (double)hr[n][i]);
-    fprintf(fo, "};\nRYS_STORAGE double rys_herm_w[%d] = {", nmax * (nmax + 1) / 2);
+    fprintf(fo, "};\nRYS_META double rys_herm_w[%d] = {", nmax * (nmax + 1) / 2);
     for (int n = 1; n <= nmax; n++)
         for (int i = 0; i < n; i++) fprintf(fo, "%s%a", (n == 1 && i == 0) ? "" : ", ", (double)hh[n][i]);
-    fprintf(fo, "};\nRYS_STORAGE double rys_coef[%d] = {\n", off[nmax + 1]);
+    fprintf(fo, "};\n#ifdef RYS_WANT_COEF\nstatic const double rys_coef[%d] = {\n", off[nmax + 1]);
     for (int n = 1; n <= nmax; n++) {
         size_t cnt = (size_t)nint[n] * 2 * n * NC;
         for (size_t k = 0; k < cnt; k++)
             fprintf(fo, "%a,%s", tables[n][k], (k % 4 == 3) ? "\n" : " ");
     }
-    fprintf(fo, "};\n");
+    fprintf(fo, "};\n#endif\n");
     fclose(fo);
     return 0;
 }

@@ -56,9 +56,11 @@ def basis_seg_contraction(mol):
             blocks.append(np.eye(nf))
             continue
         pexp, pcoeff = int(shell[gmole.PTR_EXP]), int(shell[gmole.PTR_COEFF])
-        exps = env[pexp:pexp + nprim]
+        exps = mol._env[pexp:pexp + nprim]
         norm = gmole.gto_norm(l, exps)
-        c = env[pcoeff:pcoeff + nprim * nctr].reshape(nctr, nprim) / norm
+        # atoms of one element share env slots: read the original
+        # coefficients, not the copy already rewritten for an earlier atom
+        c = mol._env[pcoeff:pcoeff + nprim * nctr].reshape(nctr, nprim) / norm
         # rows: (primitive p, component f); cols: (contraction i, component f)
         blk = np.kron(c.T, np.eye(nf))
         env[pcoeff:pcoeff + nprim] = norm

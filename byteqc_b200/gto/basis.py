@@ -11,7 +11,7 @@ Two sources are supported:
   ``standin-6-31g*``.  Each has the shell structure of the named set as PySCF
   stores it -- the same angular momenta, primitive counts and numbers of
   (general) contractions per element, hence the same number of spherical
-  functions (H2O: 24, 43 and 19) -- with even-tempered exponents over
+  functions (H2O: 24, 43 and 18) -- with even-tempered exponents over
   typical ranges and smooth synthetic contraction coefficients.  They
   exercise exactly the integral classes, contraction patterns and
   decontraction paths of the named sets; their energies are not those of

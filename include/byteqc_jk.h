@@ -101,6 +101,10 @@ int jk_get_jk(jk_basis_t *basis, const double *coeff, int nao0, const double *dm
  * host (for checking the tables).  Returns JK_ERR_ARG for n outside 1..11. */
 int jk_rys_roots_host(int n, double x, double *s, double *w);
 
+/* The same tables evaluated by a device kernel: x, s, w are device arrays
+ * (count, count*n, count*n).  For checking the device copy of the tables. */
+int jk_rys_roots_device(int n, const double *x, int count, double *s, double *w, void *stream);
+
 /* Per class quartet (8 ints each): cp_ij, cp_kl, li, lj, lk, ll, nprim_ij,
  * nprim_kl.  No reference counterpart: introspection for the cost model. */
 int jk_basis_cq_info(const jk_basis_t *basis, int *out);

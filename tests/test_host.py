@@ -1,0 +1,95 @@
+"""Host-side logic that needs no GPU: the working-basis construction, the
+stand-in basis sets, the geometry generators and the one-electron
+integrals."""
+import numpy as np
+import pytest
+
+from byteqc_b200.gto import Mole, geom, basis as gbasis
+from byteqc_b200.gto.mole import cart2sph
+
+
+@pytest.mark.parametrize('bname', ['standin-cc-pvdz', 'standin-6-31g*',
+                                   'standin-def2-tzvp'])
+def test_seg_contraction_matches_oracle(bname):
+    from byteqc_b200.cuobc.scf import hf
+    from oracle import hf_oracle
+    mol = Mole(atom=geom.water_cluster(3, box=6.0, seed=1), basis=bname).build()
+    pmol, c = hf.basis_seg_contraction(mol)
+    rmol, rc = hf_oracle.basis_seg_contraction(mol)
+    np.testing.assert_array_equal(pmol._bas, rmol._bas)
+    np.testing.assert_allclose(pmol._env, rmol._env, rtol=0, atol=0)
+    np.testing.assert_allclose(c, rc, rtol=1e-14, atol=1e-15)
+    # the working basis reproduces the contracted overlap
+    s0 = mol.intor('int1e_ovlp')
+    s1 = pmol.intor('int1e_ovlp')
+    np.testing.assert_allclose(c.T @ s1 @ c, s0, atol=1e-12)
+
+
+def test_standin_sizes():
+    # spherical functions per water: cc-pVDZ 24, def2-TZVP 43, 6-31G* 18
+    for b, n in (('standin-cc-pvdz', 24), ('standin-def2-tzvp', 43),
+                 ('standin-6-31g*', 18)):
+        assert gbasis.n_spherical(b, 'O') + 2 * gbasis.n_spherical(b, 'H') == n
+    mol = Mole(atom=geom.water_cluster(8, box=9.0, seed=0),
+               basis='standin-cc-pvdz').build()
+    assert mol.nao == 192
+    mol = Mole(atom=geom.water_cluster(32, box=14.0, seed=2),
+               basis='standin-def2-tzvp').build()
+    assert mol.nao == 1376
+
+
+def test_water_cluster_constraints():
+    atoms = geom.water_cluster(16, box=11.0, seed=5)
+    xyz = np.array([a[1] for a in atoms])
+    o = xyz[0::3]
+    d = np.linalg.norm(o[:, None] - o[None], axis=-1)
+    assert d[np.triu_indices(len(o), 1)].min() >= 2.6
+    assert (o >= 0).all() and (o <= 11.0).all()
+    for i in range(16):
+        oh1 = np.linalg.norm(xyz[3 * i + 1] - xyz[3 * i])
+        oh2 = np.linalg.norm(xyz[3 * i + 2] - xyz[3 * i])
+        ang = np.degrees(np.arccos(np.dot(xyz[3 * i + 1] - xyz[3 * i],
+                                          xyz[3 * i + 2] - xyz[3 * i])
+                                   / (oh1 * oh2)))
+        assert abs(oh1 - 0.957) < 1e-12 and abs(oh2 - 0.957) < 1e-12
+        assert abs(ang - 104.5) < 1e-9
+
+
+def test_random_walk_molecule():
+    atoms = geom.random_walk_molecule(40, seed=4)
+    xyz = np.array([a[1] for a in atoms])
+    d = np.linalg.norm(xyz[:, None] - xyz[None], axis=-1)
+    assert d[np.triu_indices(40, 1)].min() >= 1.2 - 1e-12
+    z = {'H': 1, 'C': 6, 'N': 7, 'O': 8}
+    assert sum(z[a[0]] for a in atoms) % 2 == 0
+
+
+def test_cart2sph_orthonormal():
+    # spherical functions are orthonormal on the unit sphere: check via the
+    # overlap of one normalised shell per l
+    for l in range(4):
+        mol = Mole(atom=[('H', (0, 0, 0))], basis={'H': [[l, [1.1, 1.0]]]}).build()
+        s = mol.intor('int1e_ovlp')
+        np.testing.assert_allclose(s, np.eye(2 * l + 1), atol=1e-13)
+    c = cart2sph(2)
+    # d_{xy} is sqrt(15/4pi) xy and d_{x2-y2} is sqrt(15/16pi) (x2 - y2)
+    assert abs(c[1, 0] - np.sqrt(15 / (4 * np.pi))) < 1e-14
+    assert abs(c[0, 4] - np.sqrt(15 / (16 * np.pi))) < 1e-14
+
+
+def test_scf_like_density():
+    mol = Mole(atom=geom.water_cluster(2, box=5.0, seed=0),
+               basis='standin-cc-pvdz').build()
+    s = mol.intor('int1e_ovlp')
+    d = geom.scf_like_density(s, nocc=10, seed=1)
+    # idempotent in the S metric: (D S / 2)^2 = D S / 2, trace(D S) = 2 nocc
+    ds = d @ s / 2
+    np.testing.assert_allclose(ds @ ds, ds, atol=1e-10)
+    assert abs(np.trace(d @ s) - 20) < 1e-10
+
+
+def test_one_electron_analytic():
+    a = 1.3
+    mol = Mole(atom=[('H', (0, 0, 0))], basis={'H': [[0, [a, 1.0]]]}).build()
+    assert abs(mol.intor('int1e_kin')[0, 0] - 1.5 * a) < 1e-13
+    assert abs(mol.intor('int1e_nuc')[0, 0] + 2 * np.sqrt(2 * a / np.pi)) < 1e-13

@@ -79,3 +79,25 @@ def test_pairs_and_qcond_vs_oracle():
                                atol=1e-16)
     np.testing.assert_array_equal(opt.bas_pairs_locs, ropt.bas_pairs_locs)
     np.testing.assert_allclose(opt.coeff, ropt.coeff, atol=1e-15)
+
+
+def test_device_rys_tables_match_host():
+    import torch
+    from byteqc_b200.cuobc import lib as jklib
+    lib = jklib.load_library()
+    rng = np.random.default_rng(1)
+    xs = np.concatenate([[0., 1e-13, 1.0, 2.0, 41.9, 42.0, 97.9, 200., 1e5],
+                         rng.uniform(0, 120, 200)])
+    dx = torch.as_tensor(xs, device='cuda')
+    for n in range(1, 12):
+        ds = torch.zeros(len(xs) * n, dtype=torch.float64, device='cuda')
+        dw = torch.zeros_like(ds)
+        assert lib.jk_rys_roots_device(n, dx.data_ptr(), len(xs), ds.data_ptr(),
+                                       dw.data_ptr(), None) == 0
+        s = ds.cpu().numpy().reshape(-1, n)
+        w = dw.cpu().numpy().reshape(-1, n)
+        for i, x in enumerate(xs):
+            hs, hw = np.zeros(n), np.zeros(n)
+            lib.jk_rys_roots_host(n, x, hs.ctypes.data, hw.ctypes.data)
+            np.testing.assert_allclose(s[i], hs, rtol=1e-14, atol=1e-300)
+            np.testing.assert_allclose(w[i], hw, rtol=1e-14, atol=1e-300)
