@@ -15,6 +15,7 @@
 
 #include "../../include/byteqc_jk.h"
 #include "jk_launch.cuh"
+#include "jk_internal.h"
 
 // ---------------------------------------------------------------------------
 // errors
@@ -917,5 +918,32 @@ extern "C" int jk_rys_roots_device(int n, const double* x, int count, double* s,
         default: jk_rys_eval_kernel<11><<<nb, 128, 0, st>>>(rys, x, count, s, w); break;
     }
     CUDA_TRY(cudaGetLastError());
+    return JK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// internal helpers for the other translation units
+// ---------------------------------------------------------------------------
+int jk_internal_set_err(int code, const char* msg) { return set_err(code, "%s", msg); }
+
+int jk_internal_class_info(const jk_basis_t* b, int cp_ij, int cp_kl, int* n_ij, int* n_kl, int* nao) {
+    if (!b || cp_ij < 0 || cp_ij >= b->ncp || cp_kl < 0 || cp_kl > cp_ij)
+        return set_err(JK_ERR_ARG, "bad class pair (%d, %d)", cp_ij, cp_kl);
+    *n_ij = b->h_pair_locs[cp_ij + 1] - b->h_pair_locs[cp_ij];
+    *n_kl = b->h_pair_locs[cp_kl + 1] - b->h_pair_locs[cp_kl];
+    *nao = b->nao;
+    return JK_OK;
+}
+
+void jk_internal_fill_seg(const jk_basis_t* b, int cp_ij, int cp_kl, const long long* qoff, int n_ij,
+                          const double* dm, int n_dm, double* vj, double* vk, JKSeg* out) {
+    fill_seg(b, cp_ij, cp_kl, qoff, n_ij, dm, n_dm, vj, vk, out);
+}
+
+int jk_internal_launch(const jk_basis_t* b, int cp_ij, int cp_kl, const JKSeg* d_seg, const long long* d_task0,
+                       long long max_tasks, void* stream) {
+    jk_launch_fn fn = g_tab64[class_index(b, cp_ij, cp_kl)];
+    if (!fn) return set_err(JK_ERR_UNSUPPORTED, "no kernel for class pair (%d, %d)", cp_ij, cp_kl);
+    CUDA_TRY(fn(d_seg, d_task0, 1, max_tasks, b->nsm, (cudaStream_t)stream));
     return JK_OK;
 }

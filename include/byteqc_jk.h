@@ -78,6 +78,23 @@ int jk_build_class_pair(jk_basis_t *basis, double *vj, double *vk, const double 
                         void *stream);
 
 /*
+ * Same computation and buffer contract as jk_build_class_pair, for callers
+ * that must not allocate device memory while they run (a serving process or
+ * host framework that owns all GPU memory through its own pool and cannot
+ * have a library call cudaMalloc behind it).  No counterpart in the
+ * reference.  It allocates nothing: its scratch is a fixed device array of
+ * about 1 MB inside libjk.so, held on every GPU that loads the library.
+ * Limits: at most 131072 shell pairs in the ij class and nbins <= 1024;
+ * larger requests return JK_ERR_ARG.  The first call on a device looks up the
+ * array's device address (make it before any stream capture).  All calls
+ * share the array: calls whose GPU work overlaps race and must be serialised
+ * by the caller.
+ */
+int jk_build_class_pair_noalloc(jk_basis_t *basis, double *vj, double *vk, const double *dm, int nao, int n_dm,
+                                const int *bins_locs_ij, const int *bins_locs_kl, int nbins, int cp_ij, int cp_kl,
+                                void *stream);
+
+/*
  * All class pairs in one call with the screening done on the device: the
  * per-group density condensation, the class-level density screen and the
  * log-Schwarz bin test per quartet, with the reference's decisions
