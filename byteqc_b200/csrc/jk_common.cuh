@@ -19,38 +19,184 @@
                 1.77245385090551602730)
 
 // ---------------------------------------------------------------------------
-// Rys nodes s_r = t_r^2 and weights w_r at x = rho |P-Q|^2 from the generated
-// Chebyshev tables (uniform intervals of width rys_h[n] up to rys_xmax[n],
-// Gauss-Hermite limit beyond).  The reference evaluates the same quantities
-// in the variable u = t^2/(1-t^2) (cuobc/lib/gint/rys_roots.cu:1214-2176).
+// Rys nodes s_r = t_r^2 and weights w_r at x = rho |P-Q|^2.  The reference
+// evaluates the same quantities in the variable u = t^2/(1-t^2)
+// (cuobc/lib/gint/rys_roots.cu:1214-2176).
+//   n = 1:  w = F0(x), s = F1(x)/F0(x) from the Boys function itself
+//           (a Taylor series below x = 0.75, erf/exp above);
+//   n > 1:  the generated Chebyshev tables (uniform intervals of width 2 up
+//           to rys_xmax[n], Gauss-Hermite limit beyond), evaluated from a
+//           copy of the n-root table in shared memory.  Lanes of a warp
+//           read the intervals of their own x; the copy's interval stride is
+//           odd in doubles so that different intervals start in different
+//           banks.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double rys_cheb(const double* __restrict__ c, double t) {
-    double b1 = 0., b2 = 0., t2 = t + t;
-#pragma unroll
-    for (int k = RYS_NC - 1; k >= 1; k--) {
-        double b0 = fma(t2, b1, __ldg(c + k) - b2);
-        b2 = b1;
-        b1 = b0;
+template <int N>
+struct RysS {
+    static constexpr int NS = 2 * N;                 // series per interval
+    static constexpr int STRIDE = NS * RYS_NC + 1;   // doubles per interval
+    static constexpr int NINT = rys_nint_c(N);
+    static constexpr int HERM = NINT * STRIDE;       // Gauss-Hermite nodes, then weights
+    static constexpr int WORDS = N == 1 ? 0 : HERM + NS;  // doubles in shared memory
+    static constexpr double XMAX = rys_xmax_c(N);
+};
+
+// block-cooperative copy of the n-root table into shared memory (layout
+// [interval][k][series], series f < N nodes, f >= N weights)
+template <int N>
+__device__ __forceinline__ void rys_table_to_smem(const double* __restrict__ g, double* __restrict__ tab) {
+    using S = RysS<N>;
+    if (N == 1) return;
+    const double* src = g + rys_off_c(N);
+    for (int e = threadIdx.x; e < S::NINT * S::NS * RYS_NC; e += blockDim.x) {
+        int m = e / (S::NS * RYS_NC);
+        int rem = e - m * (S::NS * RYS_NC);
+        int f = rem / RYS_NC, k = rem - f * RYS_NC;
+        tab[m * S::STRIDE + k * S::NS + f] = __ldg(src + e);
     }
-    return fma(t, b1, __ldg(c) - b2);
+    for (int r = threadIdx.x; r < N; r += blockDim.x) {
+        tab[S::HERM + r] = rys_herm_r[N * (N - 1) / 2 + r];
+        tab[S::HERM + N + r] = rys_herm_w[N * (N - 1) / 2 + r];
+    }
 }
 
+// F0 and F1 of the Boys function
+__device__ __forceinline__ void boys01(double x, double& f0, double& f1) {
+    if (x < 0.75) {
+        // F_m(x) = sum_k (-x)^k / (k! (2m + 2k + 1)), 19 terms (< 1e-18 at 0.75)
+        double a0 = 0., a1 = 0., fk = 1.;
+        double c0[19], c1[19];
+#pragma unroll
+        for (int k = 0; k < 19; k++) {
+            if (k) fk *= k;
+            c0[k] = ((k & 1) ? -1. : 1.) / (fk * (2 * k + 1));
+            c1[k] = ((k & 1) ? -1. : 1.) / (fk * (2 * k + 3));
+        }
+#pragma unroll
+        for (int k = 18; k >= 0; k--) {
+            a0 = fma(a0, x, c0[k]);
+            a1 = fma(a1, x, c1[k]);
+        }
+        f0 = a0;
+        f1 = a1;
+    } else {
+        double sx = sqrt(x);
+        f0 = 0.88622692545275801365 * erf(sx) / sx;  // sqrt(pi)/2 erf(sqrt x)/sqrt x
+        f1 = (f0 - exp(-x)) / (2. * x);
+    }
+}
+
+// all N roots at x from the shared-memory table
+template <int N>
+__device__ __forceinline__ void rys_roots_all(const double* __restrict__ tab, double x, double* s, double* w) {
+    using S = RysS<N>;
+    if (N == 1) {
+        double f0, f1;
+        boys01(x, f0, f1);
+        w[0] = f0;
+        s[0] = f1 / f0;
+        return;
+    }
+    if (x >= S::XMAX) {
+        double rx = 1. / x, srx = sqrt(rx);
+#pragma unroll
+        for (int r = 0; r < N; r++) {
+            s[r] = tab[S::HERM + r] * rx;
+            w[r] = tab[S::HERM + N + r] * srx;
+        }
+        return;
+    }
+    int m = (int)(x * 0.5);
+    double t = x - (2 * m + 1), t2 = t + t;
+    const double* c = tab + m * S::STRIDE;
+    double b1[S::NS], b2[S::NS];
+#pragma unroll
+    for (int f = 0; f < S::NS; f++) b1[f] = b2[f] = 0.;
+#pragma unroll
+    for (int k = RYS_NC - 1; k >= 1; k--) {
+#pragma unroll
+        for (int f = 0; f < S::NS; f++) {
+            double b0 = fma(t2, b1[f], c[k * S::NS + f] - b2[f]);
+            b2[f] = b1[f];
+            b1[f] = b0;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < N; r++) {
+        s[r] = fma(t, b1[r], c[r] - b2[r]);
+        w[r] = fma(t, b1[N + r], c[N + r] - b2[N + r]);
+    }
+}
+
+// root r only (runtime r) from the shared-memory table
+template <int N>
+__device__ __forceinline__ void rys_root_one(const double* __restrict__ tab, double x, int r, double& s, double& w) {
+    using S = RysS<N>;
+    if (N == 1) {
+        double f0, f1;
+        boys01(x, f0, f1);
+        w = f0;
+        s = f1 / f0;
+        return;
+    }
+    if (x >= S::XMAX) {
+        double rx = 1. / x;
+        s = tab[S::HERM + r] * rx;
+        w = tab[S::HERM + N + r] * sqrt(rx);
+        return;
+    }
+    int m = (int)(x * 0.5);
+    double t = x - (2 * m + 1), t2 = t + t;
+    const double* c = tab + m * S::STRIDE;
+    double bs1 = 0., bs2 = 0., bw1 = 0., bw2 = 0.;
+#pragma unroll
+    for (int k = RYS_NC - 1; k >= 1; k--) {
+        double b0 = fma(t2, bs1, c[k * S::NS + r] - bs2);
+        bs2 = bs1;
+        bs1 = b0;
+        b0 = fma(t2, bw1, c[k * S::NS + N + r] - bw2);
+        bw2 = bw1;
+        bw1 = b0;
+    }
+    s = fma(t, bs1, c[r] - bs2);
+    w = fma(t, bw1, c[N + r] - bw2);
+}
+
+// root r straight from the global table (setup kernels)
 template <int N>
 __device__ __forceinline__ void rys_root(const double* __restrict__ rys_coef, double x, int r, double& s,
                                          double& w) {
-    if (x >= rys_xmax[N]) {
+    if (N == 1) {
+        double f0, f1;
+        boys01(x, f0, f1);
+        w = f0;
+        s = f1 / f0;
+        return;
+    }
+    if (x >= rys_xmax_c(N)) {
         int b = N * (N - 1) / 2 + r;
         double rx = 1. / x;
         s = rys_herm_r[b] * rx;
         w = rys_herm_w[b] * sqrt(rx);
         return;
     }
-    // rys_h is 2 for every n (checked by the host at load time)
     int m = (int)(x * 0.5);
     double t = x - (2 * m + 1);
-    const double* c = rys_coef + rys_off[N] + (m * 2 * N) * RYS_NC;
-    s = rys_cheb(c + r * RYS_NC, t);
-    w = rys_cheb(c + (N + r) * RYS_NC, t);
+    const double* c = rys_coef + rys_off_c(N) + (m * 2 * N) * RYS_NC;
+    double b1 = 0., b2 = 0., v1 = 0., v2 = 0., tt = t + t;
+    const double* cs = c + r * RYS_NC;
+    const double* cw = c + (N + r) * RYS_NC;
+#pragma unroll
+    for (int k = RYS_NC - 1; k >= 1; k--) {
+        double b0 = fma(tt, b1, __ldg(cs + k) - b2);
+        b2 = b1;
+        b1 = b0;
+        b0 = fma(tt, v1, __ldg(cw + k) - v2);
+        v2 = v1;
+        v1 = b0;
+    }
+    s = fma(t, b1, __ldg(cs) - b2);
+    w = fma(t, v1, __ldg(cw) - v2);
 }
 
 // ---------------------------------------------------------------------------
@@ -58,25 +204,16 @@ __device__ __forceinline__ void rys_root(const double* __restrict__ rys_coef, do
 // ---------------------------------------------------------------------------
 __host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
 
-// x and y exponents of Cartesian component c of angular momentum l in libcint
-// order (lx descending, then ly descending)
-__host__ __device__ constexpr int cart_lx(int l, int c) {
-    int lx = l;
-    while (c > l - lx) {
-        c -= l - lx + 1;
-        lx--;
-    }
-    return lx;
+// Exponents of Cartesian component c of angular momentum l in libcint order
+// (lx descending, then ly descending).  With u = l - lx, the components with
+// x exponent above lx number u(u+1)/2, so u is the triangular root of c and
+// lz = c - u(u+1)/2.  Loop-free so that unrolled loops fold them to constants.
+__host__ __device__ constexpr int cart_u(int c) {
+    return c < 1 ? 0 : c < 3 ? 1 : c < 6 ? 2 : c < 10 ? 3 : c < 15 ? 4 : c < 21 ? 5 : 6;
 }
-__host__ __device__ constexpr int cart_ly(int l, int c) {
-    int lx = l;
-    while (c > l - lx) {
-        c -= l - lx + 1;
-        lx--;
-    }
-    return l - lx - c;
-}
-__host__ __device__ constexpr int cart_lz(int l, int c) { return l - cart_lx(l, c) - cart_ly(l, c); }
+__host__ __device__ constexpr int cart_lz(int l, int c) { return c - cart_u(c) * (cart_u(c) + 1) / 2; }
+__host__ __device__ constexpr int cart_lx(int l, int c) { return l - cart_u(c); }
+__host__ __device__ constexpr int cart_ly(int l, int c) { return cart_u(c) - cart_lz(l, c); }
 
 template <int LI_, int LJ_, int LK_, int LL_>
 struct JKClass {
@@ -90,9 +227,14 @@ struct JKClass {
     static constexpr int GS = (LI + 1) * SI;
     // ownership: P leading centres are owned by a thread of the team; the
     // remaining Cartesian components are accumulated in registers
-    static constexpr int P = (NF <= 64) ? 0 : ((NF / NFI <= 64) ? 1 : 2);
+    // one thread per quartet when its accumulators and one root's 2D blocks
+    // fit in registers (W doubles), else a team
+    static constexpr int W = NF + 3 * GS;
+    static constexpr int P = (W <= 64) ? 0 : ((NF / NFI <= 64) ? 1 : 2);
     static constexpr int T = P == 0 ? 1 : (P == 1 ? NFI : NFI * NFJ);
     static constexpr int NACC = NF / T;
+    // resident 128-thread blocks asked of the register allocator (thread kernel)
+    static constexpr int MINB = W <= 24 ? 4 : (W <= 40 ? 3 : 2);
 };
 
 // ---------------------------------------------------------------------------

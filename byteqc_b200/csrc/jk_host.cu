@@ -308,16 +308,12 @@ struct jk_basis {
     JKScreenCQ* d_cq = nullptr;
     long long *d_qoff = nullptr, *d_task0 = nullptr;
     double* d_dm_cond = nullptr;
-    JKSeg* d_seg = nullptr;
-    JKSeg* h_seg = nullptr;  // pinned
     // reference-compatible single class-pair path
     long long* d_qoff1 = nullptr;
     long long* d_task01 = nullptr;
     long long qoff1_cap = 0;
     long long* h_qoff1 = nullptr;  // pinned
     size_t h_qoff1_cap = 0;
-    JKSeg* d_seg1 = nullptr;
-    JKSeg* h_seg1 = nullptr;
     // transform workspace
     cublasHandle_t blas = nullptr;
     double* d_work = nullptr;
@@ -341,13 +337,9 @@ static void free_basis(jk_basis* b) {
     cudaFree(b->d_qoff);
     cudaFree(b->d_task0);
     cudaFree(b->d_dm_cond);
-    cudaFree(b->d_seg);
     cudaFree(b->d_qoff1);
     cudaFree(b->d_task01);
-    cudaFree(b->d_seg1);
     cudaFree(b->d_work);
-    if (b->h_seg) cudaFreeHost(b->h_seg);
-    if (b->h_seg1) cudaFreeHost(b->h_seg1);
     if (b->h_qoff1) cudaFreeHost(b->h_qoff1);
     if (b->blas) cublasDestroy(b->blas);
     delete b;
@@ -572,10 +564,6 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
     CUDA_TRY(cudaMalloc(&b->d_qoff, sizeof(long long) * (b->qoff_total ? b->qoff_total : 1)));
     CUDA_TRY(cudaMalloc(&b->d_task0, sizeof(long long) * 2 * (b->ncq ? b->ncq : 1)));
     CUDA_TRY(cudaMalloc(&b->d_dm_cond, sizeof(double) * ngroups * ngroups));
-    CUDA_TRY(cudaMalloc(&b->d_seg, sizeof(JKSeg) * (b->ncq ? b->ncq : 1)));
-    CUDA_TRY(cudaMallocHost(&b->h_seg, sizeof(JKSeg) * (b->ncq ? b->ncq : 1)));
-    CUDA_TRY(cudaMalloc(&b->d_seg1, sizeof(JKSeg)));
-    CUDA_TRY(cudaMallocHost(&b->h_seg1, sizeof(JKSeg)));
     CUDA_TRY(cudaMalloc(&b->d_task01, sizeof(long long) * 2));
     return JK_OK;
 }
@@ -678,19 +666,14 @@ extern "C" int jk_build(jk_basis_t* b, const double* dm, int n_dm, double* vj, d
     CUDA_TRY(cudaGetLastError());
     for (int c = 0; c < b->ncq; c++) {
         const JKScreenCQ& cq = b->h_cq[c];
-        fill_seg(b, cq.cp_ij, cq.cp_kl, b->d_qoff + cq.qoff_off, cq.n_ij, dm, n_dm, vj, vk, b->h_seg + c);
-    }
-    CUDA_TRY(cudaMemcpyAsync(b->d_seg, b->h_seg, sizeof(JKSeg) * b->ncq, cudaMemcpyHostToDevice, st));
-    for (int c = 0; c < b->ncq; c++) {
-        const JKScreenCQ& cq = b->h_cq[c];
+        JKSeg seg;
+        fill_seg(b, cq.cp_ij, cq.cp_kl, b->d_qoff + cq.qoff_off, cq.n_ij, dm, n_dm, vj, vk, &seg);
         long long maxt = cq.cp_ij == cq.cp_kl ? (long long)cq.n_ij * (cq.n_ij + 1) / 2
                                               : (long long)cq.n_ij * cq.n_kl;
         jk_launch_fn fn = g_tab64[class_index(b, cq.cp_ij, cq.cp_kl)];
         if (!fn) return set_err(JK_ERR_UNSUPPORTED, "no kernel for class quartet %d", c);
-        CUDA_TRY(fn(b->d_seg + c, b->d_task0 + 2 * c, 1, maxt, b->nsm, st));
+        CUDA_TRY(fn(seg, b->d_task0 + 2 * c, maxt, b->nsm, st));
     }
-    // the pinned segment table must not be rewritten before the copy ran
-    CUDA_TRY(cudaStreamSynchronize(st));
     return JK_OK;
 }
 
@@ -734,11 +717,11 @@ extern "C" int jk_build_class_pair(jk_basis_t* b, double* vj, double* vk, const 
     CUDA_TRY(cudaMemcpyAsync(b->d_qoff1, qo, sizeof(long long) * (n_ij + 1), cudaMemcpyHostToDevice, st));
     long long t0[2] = {0, tot};
     CUDA_TRY(cudaMemcpyAsync(b->d_task01, t0, sizeof(t0), cudaMemcpyHostToDevice, st));
-    fill_seg(b, cp_ij, cp_kl, b->d_qoff1, n_ij, dm, n_dm, vj, vk, b->h_seg1);
-    CUDA_TRY(cudaMemcpyAsync(b->d_seg1, b->h_seg1, sizeof(JKSeg), cudaMemcpyHostToDevice, st));
+    JKSeg seg;
+    fill_seg(b, cp_ij, cp_kl, b->d_qoff1, n_ij, dm, n_dm, vj, vk, &seg);
     jk_launch_fn fn = g_tab64[class_index(b, cp_ij, cp_kl)];
     if (!fn) return set_err(JK_ERR_UNSUPPORTED, "no kernel for this class pair");
-    CUDA_TRY(fn(b->d_seg1, b->d_task01, 1, tot, b->nsm, st));
+    CUDA_TRY(fn(seg, b->d_task01, tot, b->nsm, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     return JK_OK;
 }
@@ -887,37 +870,65 @@ extern "C" int jk_fma_peak(int fp32, double* tflops) {
     return JK_OK;
 }
 
-// device evaluation of the Rys tables at a batch of points (checks the
-// device copy of the tables against the host evaluation)
+// device evaluation of the Rys tables at a batch of points, through the
+// paths the kernels use: mode 0 all roots from the shared-memory copy (thread
+// kernels), 1 one root at a time from it (team kernels), 2 one root from the
+// global table (setup kernels)
 template <int N>
-__global__ void jk_rys_eval_kernel(const double* rys, const double* x, int count, double* s, double* w) {
+__global__ void jk_rys_eval_kernel(const double* rys, const double* x, int count, double* s, double* w, int mode) {
+    extern __shared__ __align__(16) double tab[];
+    rys_table_to_smem<N>(rys, tab);
+    __syncthreads();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
-    for (int r = 0; r < N; r++) rys_root<N>(rys, x[i], r, s[i * N + r], w[i * N + r]);
+    if (mode == 0) {
+        double rs[N], rw[N];
+        rys_roots_all<N>(tab, x[i], rs, rw);
+        for (int r = 0; r < N; r++) {
+            s[i * N + r] = rs[r];
+            w[i * N + r] = rw[r];
+        }
+    } else {
+        for (int r = 0; r < N; r++) {
+            if (mode == 1) rys_root_one<N>(tab, x[i], r, s[i * N + r], w[i * N + r]);
+            else rys_root<N>(rys, x[i], r, s[i * N + r], w[i * N + r]);
+        }
+    }
 }
 
-extern "C" int jk_rys_roots_device(int n, const double* x, int count, double* s, double* w, void* stream) {
-    if (n < 1 || n > 11 || !x || !s || !w || count < 0) return set_err(JK_ERR_ARG, "jk_rys_roots_device: bad args");
+template <int N>
+static cudaError_t rys_eval_launch(const double* rys, const double* x, int count, double* s, double* w, int mode,
+                                   cudaStream_t st) {
+    size_t smem = RysS<N>::WORDS * sizeof(double);
+    cudaError_t e = cudaFuncSetAttribute(jk_rys_eval_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    jk_rys_eval_kernel<N><<<(count + 127) / 128, 128, smem, st>>>(rys, x, count, s, w, mode);
+    return cudaGetLastError();
+}
+
+extern "C" int jk_rys_roots_device(int n, const double* x, int count, double* s, double* w, int mode, void* stream) {
+    if (n < 1 || n > 11 || !x || !s || !w || count < 0 || mode < 0 || mode > 2)
+        return set_err(JK_ERR_ARG, "jk_rys_roots_device: bad args");
     if (count == 0) return JK_OK;
     const double* rys;
     int rc = rys_table_device(&rys);
     if (rc) return rc;
     cudaStream_t st = (cudaStream_t)stream;
-    int nb = (count + 127) / 128;
+    cudaError_t e;
     switch (n) {
-        case 1: jk_rys_eval_kernel<1><<<nb, 128, 0, st>>>(rys, x, count, s, w); break;
-        case 2: jk_rys_eval_kernel<2><<<nb, 128, 0, st>>>(rys, x, count, s, w); break;
-        case 3: jk_rys_eval_kernel<3><<<nb, 128, 0, st>>>(rys, x, count, s, w); break;
-        case 4: jk_rys_eval_kernel<4><<<nb, 128, 0, st>>>(rys, x, count, s, w); break;
-        case 5: jk_rys_eval_kernel<5><<<nb, 128, 0, st>>>(rys, x, count, s, w); break;
-        case 6: jk_rys_eval_kernel<6><<<nb, 128, 0, st>>>(rys, x, count, s, w); break;
-        case 7: jk_rys_eval_kernel<7><<<nb, 128, 0, st>>>(rys, x, count, s, w); break;
-        case 8: jk_rys_eval_kernel<8><<<nb, 128, 0, st>>>(rys, x, count, s, w); break;
-        case 9: jk_rys_eval_kernel<9><<<nb, 128, 0, st>>>(rys, x, count, s, w); break;
-        case 10: jk_rys_eval_kernel<10><<<nb, 128, 0, st>>>(rys, x, count, s, w); break;
-        default: jk_rys_eval_kernel<11><<<nb, 128, 0, st>>>(rys, x, count, s, w); break;
+        case 1: e = rys_eval_launch<1>(rys, x, count, s, w, mode, st); break;
+        case 2: e = rys_eval_launch<2>(rys, x, count, s, w, mode, st); break;
+        case 3: e = rys_eval_launch<3>(rys, x, count, s, w, mode, st); break;
+        case 4: e = rys_eval_launch<4>(rys, x, count, s, w, mode, st); break;
+        case 5: e = rys_eval_launch<5>(rys, x, count, s, w, mode, st); break;
+        case 6: e = rys_eval_launch<6>(rys, x, count, s, w, mode, st); break;
+        case 7: e = rys_eval_launch<7>(rys, x, count, s, w, mode, st); break;
+        case 8: e = rys_eval_launch<8>(rys, x, count, s, w, mode, st); break;
+        case 9: e = rys_eval_launch<9>(rys, x, count, s, w, mode, st); break;
+        case 10: e = rys_eval_launch<10>(rys, x, count, s, w, mode, st); break;
+        default: e = rys_eval_launch<11>(rys, x, count, s, w, mode, st); break;
     }
-    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(e);
     return JK_OK;
 }
 
@@ -940,10 +951,10 @@ void jk_internal_fill_seg(const jk_basis_t* b, int cp_ij, int cp_kl, const long 
     fill_seg(b, cp_ij, cp_kl, qoff, n_ij, dm, n_dm, vj, vk, out);
 }
 
-int jk_internal_launch(const jk_basis_t* b, int cp_ij, int cp_kl, const JKSeg* d_seg, const long long* d_task0,
+int jk_internal_launch(const jk_basis_t* b, int cp_ij, int cp_kl, const JKSeg& seg, const long long* d_task0,
                        long long max_tasks, void* stream) {
     jk_launch_fn fn = g_tab64[class_index(b, cp_ij, cp_kl)];
     if (!fn) return set_err(JK_ERR_UNSUPPORTED, "no kernel for class pair (%d, %d)", cp_ij, cp_kl);
-    CUDA_TRY(fn(d_seg, d_task0, 1, max_tasks, b->nsm, (cudaStream_t)stream));
+    CUDA_TRY(fn(seg, d_task0, max_tasks, b->nsm, (cudaStream_t)stream));
     return JK_OK;
 }

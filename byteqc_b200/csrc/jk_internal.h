@@ -10,5 +10,5 @@ int jk_internal_class_info(const jk_basis_t* b, int cp_ij, int cp_kl, int* n_ij,
 void jk_internal_fill_seg(const jk_basis_t* b, int cp_ij, int cp_kl, const long long* qoff, int n_ij,
                           const double* dm, int n_dm, double* vj, double* vk, JKSeg* out);
 // launch the class kernel of (cp_ij, cp_kl) on a device segment table of one entry
-int jk_internal_launch(const jk_basis_t* b, int cp_ij, int cp_kl, const JKSeg* d_seg, const long long* d_task0,
+int jk_internal_launch(const jk_basis_t* b, int cp_ij, int cp_kl, const JKSeg& seg, const long long* d_task0,
                        long long max_tasks, void* stream);

@@ -121,7 +121,7 @@ __device__ __forceinline__ void load_center(const JKSeg& sg, int sh, double* r) 
 // P = 0: one thread per quartet
 // ===========================================================================
 template <class C, typename R>
-__device__ __forceinline__ void jk_thread_quartet(const JKSeg& sg, const JKQuartet& q) {
+__device__ __forceinline__ void jk_thread_quartet(const JKSeg& sg, const JKQuartet& q, const double* __restrict__ tab) {
     constexpr int NR = C::NROOTS;
     double ri[3], rj[3], rk[3], rl[3];
     load_center(sg, q.ish, ri);
@@ -134,10 +134,11 @@ __device__ __forceinline__ void jk_thread_quartet(const JKSeg& sg, const JKQuart
     for (int ip = 0; ip < sg.nprim_ij; ip++)
         for (int kp = 0; kp < sg.nprim_kl; kp++) {
             JKPrim p = jk_prim(sg, q.prim_ij + ip, q.prim_kl + kp);
+            double rs[NR], rw[NR];
+            rys_roots_all<NR>(tab, p.x, rs, rw);
 #pragma unroll
             for (int r = 0; r < NR; r++) {
-                double s, w;
-                rys_root<NR>(sg.rys, p.x, r, s, w);
+                const double s = rs[r], w = rw[r];
                 R Ix[C::GS], Iy[C::GS], Iz[C::GS];
                 jk_unit<C, R>(p, s, w, 0, q.norm, ri, rj, rk, rl, Ix);
                 jk_unit<C, R>(p, s, w, 1, q.norm, ri, rj, rk, rl, Iy);
@@ -243,15 +244,16 @@ __device__ __forceinline__ void jk_thread_quartet(const JKSeg& sg, const JKQuart
 }
 
 template <class C, typename R>
-__global__ void __launch_bounds__(128) jk_thread_kernel(const JKSeg* __restrict__ segs,
-                                                        const long long* __restrict__ task0, int nseg) {
-    long long total = task0[nseg];
-    long long stride = (long long)gridDim.x * blockDim.x;
+__global__ void __launch_bounds__(128, C::MINB) jk_thread_kernel(const __grid_constant__ JKSeg sg,
+                                                                 const long long* __restrict__ task0) {
+    extern __shared__ __align__(16) double jk_tab[];
+    rys_table_to_smem<C::NROOTS>(sg.rys, jk_tab);
+    __syncthreads();
+    const long long total = task0[1];
+    const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
-        int s = jk_find_seg(task0, nseg, t);
-        JKSeg sg = segs[s];
-        JKQuartet q = jk_decode(sg, t - task0[s]);
-        jk_thread_quartet<C, R>(sg, q);
+        JKQuartet q = jk_decode(sg, t);
+        jk_thread_quartet<C, R>(sg, q, jk_tab);
     }
 }
 
@@ -262,28 +264,40 @@ template <class C>
 struct JKTeamShape {
     static constexpr int QPB = (C::T >= 128) ? 1 : (128 / C::T);  // quartets per block
     static constexpr int THREADS = QPB * C::T;
-    static constexpr int GWORDS = (3 * C::NROOTS * C::GS + 1) & ~1;  // 2D blocks per quartet (even)
-    static constexpr int BWORDS = C::NFI * C::NFJ + C::NFK * C::NFL + C::NFI * C::NFK + C::NFI * C::NFL +
-                                  C::NFJ * C::NFK + C::NFJ * C::NFL;  // digestion buffers
+    // per-team strides are odd so that teams start in different banks
+    static constexpr int GWORDS = (3 * C::NROOTS * C::GS) | 1;  // 2D blocks per quartet
+    static constexpr int BWORDS_RAW = C::NFI * C::NFJ + C::NFK * C::NFL + C::NFI * C::NFK + C::NFI * C::NFL +
+                                      C::NFJ * C::NFK + C::NFJ * C::NFL;  // digestion buffers
+    static constexpr int BWORDS = BWORDS_RAW | 1;
+    static constexpr int TAB = RysS<C::NROOTS>::WORDS;  // Rys table (doubles), first in shared memory
     static constexpr int OFF_JIJ = 0, OFF_JKL = OFF_JIJ + C::NFI * C::NFJ, OFF_KIK = OFF_JKL + C::NFK * C::NFL,
                          OFF_KIL = OFF_KIK + C::NFI * C::NFK, OFF_KJK = OFF_KIL + C::NFI * C::NFL,
                          OFF_KJL = OFF_KJK + C::NFJ * C::NFK;
 };
 
 template <class C, typename R>
-constexpr size_t jk_team_smem() {
+__host__ __device__ constexpr size_t jk_team_gbytes() {
     using S = JKTeamShape<C>;
-    return (size_t)S::QPB * (S::GWORDS * sizeof(R) + S::BWORDS * sizeof(double));
+    return ((size_t)S::QPB * S::GWORDS * sizeof(R) + 15) & ~(size_t)15;
 }
 
 template <class C, typename R>
-__global__ void jk_team_kernel(const JKSeg* __restrict__ segs, const long long* __restrict__ task0, int nseg) {
+__host__ __device__ constexpr size_t jk_team_smem() {
+    using S = JKTeamShape<C>;
+    return (size_t)S::TAB * sizeof(double) + jk_team_gbytes<C, R>() + (size_t)S::QPB * S::BWORDS * sizeof(double);
+}
+
+template <class C, typename R>
+__global__ void jk_team_kernel(const __grid_constant__ JKSeg sg0, const long long* __restrict__ task0) {
     using S = JKTeamShape<C>;
     constexpr int T = C::T, NR = C::NROOTS;
     extern __shared__ __align__(16) unsigned char jk_smem[];
     const int team = threadIdx.x / T, lane = threadIdx.x - team * T;
-    R* g = reinterpret_cast<R*>(jk_smem) + (size_t)team * S::GWORDS;
-    double* buf = reinterpret_cast<double*>(jk_smem + (size_t)S::QPB * S::GWORDS * sizeof(R)) + (size_t)team * S::BWORDS;
+    double* tab = reinterpret_cast<double*>(jk_smem);
+    unsigned char* gbase = jk_smem + (size_t)S::TAB * sizeof(double);
+    R* g = reinterpret_cast<R*>(gbase) + (size_t)team * S::GWORDS;
+    double* buf = reinterpret_cast<double*>(gbase + jk_team_gbytes<C, R>()) + (size_t)team * S::BWORDS;
+    rys_table_to_smem<NR>(sg0.rys, tab);
 
     // owned Cartesian indices
     int ci = 0, cj = 0;
@@ -299,19 +313,18 @@ __global__ void jk_team_kernel(const JKSeg* __restrict__ segs, const long long* 
         own_z += cart_lz(C::LJ, cj) * C::SJ;
     }
 
-    const long long total = task0[nseg];
+    __syncthreads();
+    const JKSeg& sg = sg0;
+    const long long total = task0[1];
     const long long nteams = (long long)gridDim.x * S::QPB;
-    const int nprim_ij = segs[0].nprim_ij, nprim_kl = segs[0].nprim_kl;  // uniform within a launch
+    const int nprim_ij = sg.nprim_ij, nprim_kl = sg.nprim_kl;
     for (long long base = (long long)blockIdx.x * S::QPB; base < total; base += nteams) {
         const long long t = base + team;
         const bool active = t < total;
-        JKSeg sg;
         JKQuartet q;
         double ri[3], rj[3], rk[3], rl[3];
         if (active) {
-            int s = jk_find_seg(task0, nseg, t);
-            sg = segs[s];
-            q = jk_decode(sg, t - task0[s]);
+            q = jk_decode(sg, t);
             load_center(sg, q.ish, ri);
             load_center(sg, q.jsh, rj);
             load_center(sg, q.ksh, rk);
@@ -327,7 +340,7 @@ __global__ void jk_team_kernel(const JKSeg* __restrict__ segs, const long long* 
                     for (int u = lane; u < 3 * NR; u += T) {
                         int r = u / 3, d = u - 3 * r;
                         double s, w;
-                        rys_root<NR>(sg.rys, p.x, r, s, w);
+                        rys_root_one<NR>(tab, p.x, r, s, w);
                         jk_unit<C, R>(p, s, w, d, q.norm, ri, rj, rk, rl, g + u * C::GS);
                     }
                 }
@@ -368,7 +381,7 @@ __global__ void jk_team_kernel(const JKSeg* __restrict__ segs, const long long* 
             }
 
         // ---- digestion ----
-        const int n_dm = active ? sg.n_dm : segs[0].n_dm;
+        const int n_dm = sg.n_dm;
         for (int idm = 0; idm < n_dm; idm++) {
             for (int e = lane; e < S::BWORDS; e += T) buf[e] = 0.;
             __syncthreads();

@@ -3,19 +3,28 @@
 #pragma once
 #include "jk_kernels.cuh"
 
-typedef cudaError_t (*jk_launch_fn)(const JKSeg* segs, const long long* task0, int nseg, long long max_tasks,
-                                    int nsm, cudaStream_t st);
+typedef cudaError_t (*jk_launch_fn)(const JKSeg& seg, const long long* task0, long long max_tasks, int nsm,
+                                    cudaStream_t st);
 
+// One class quartet (one segment): the segment descriptor goes by value into
+// the kernel's parameter space; task0[1] (device) holds the task count.
 template <int LI, int LJ, int LK, int LL, typename R>
-cudaError_t jk_launch(const JKSeg* segs, const long long* task0, int nseg, long long max_tasks, int nsm,
-                      cudaStream_t st) {
+cudaError_t jk_launch(const JKSeg& seg, const long long* task0, long long max_tasks, int nsm, cudaStream_t st) {
     using C = JKClass<LI, LJ, LK, LL>;
     if (max_tasks <= 0) return cudaSuccess;
     if constexpr (C::P == 0) {
+        constexpr size_t smem = RysS<C::NROOTS>::WORDS * sizeof(double);
+        static bool attr_set = false;
+        if (!attr_set) {
+            cudaError_t e = cudaFuncSetAttribute(jk_thread_kernel<C, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+            if (e != cudaSuccess) return e;
+            attr_set = true;
+        }
         long long want = (max_tasks + 127) / 128;
         long long cap = (long long)nsm * 16;
         int blocks = (int)(want < cap ? want : cap);
-        jk_thread_kernel<C, R><<<blocks, 128, 0, st>>>(segs, task0, nseg);
+        jk_thread_kernel<C, R><<<blocks, 128, smem, st>>>(seg, task0);
     } else {
         using S = JKTeamShape<C>;
         constexpr size_t smem = jk_team_smem<C, R>();
@@ -29,7 +38,7 @@ cudaError_t jk_launch(const JKSeg* segs, const long long* task0, int nseg, long 
         long long want = (max_tasks + S::QPB - 1) / S::QPB;
         long long cap = (long long)nsm * 8;
         int blocks = (int)(want < cap ? want : cap);
-        jk_team_kernel<C, R><<<blocks, S::THREADS, smem, st>>>(segs, task0, nseg);
+        jk_team_kernel<C, R><<<blocks, S::THREADS, smem, st>>>(seg, task0);
     }
     return cudaGetLastError();
 }

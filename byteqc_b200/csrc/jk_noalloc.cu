@@ -10,8 +10,7 @@
 // allocates its row-offset and segment buffers on first use and grows them
 // when a larger class pair comes; this entry point never does.
 //
-// How: the scratch (row offsets, task counts, the bins and the segment
-// descriptor) lives in the file-scope array jk_na_scratch below, sized for at
+// How: the scratch (row offsets, task counts and the bins) lives in the file-scope array jk_na_scratch below, sized for at
 // most JK_NA_MAX_ROWS shell pairs in the ij class and JK_NA_MAX_BINS bins.
 // Every GPU that loads libjk.so holds this array (about 1 MB) until the
 // process exits.  Host code cannot use the array's name as a device address
@@ -29,14 +28,12 @@
 #define JK_NA_MAX_ROWS (1 << 17)  // shell pairs of the ij class
 #define JK_NA_MAX_BINS 1024
 #define JK_NA_OFF_TASK0 0
-#define JK_NA_OFF_SEG 256
-#define JK_NA_OFF_BINS 1024
+#define JK_NA_OFF_BINS 256
 #define JK_NA_OFF_QOFF (JK_NA_OFF_BINS + 2 * (JK_NA_MAX_BINS + 1) * 4 + 256)
 #define JK_NA_BYTES (JK_NA_OFF_QOFF + (JK_NA_MAX_ROWS + 1) * 8)
 
 static __device__ __align__(256) unsigned char jk_na_scratch[JK_NA_BYTES];
 
-static_assert(sizeof(JKSeg) <= JK_NA_OFF_BINS - JK_NA_OFF_SEG, "segment slot too small");
 static_assert(JK_NA_OFF_QOFF % 8 == 0, "qoff alignment");
 
 static std::mutex g_na_mu;
@@ -136,22 +133,20 @@ extern "C" int jk_build_class_pair_noalloc(jk_basis_t* b, double* vj, double* vk
     if (rc) return rc;
     cudaStream_t st = (cudaStream_t)stream;
     long long* d_task0 = (long long*)(sc + JK_NA_OFF_TASK0);
-    JKSeg* d_seg = (JKSeg*)(sc + JK_NA_OFF_SEG);
     int* d_bins_ij = (int*)(sc + JK_NA_OFF_BINS);
     int* d_bins_kl = d_bins_ij + (nbins + 1);
     long long* d_qoff = (long long*)(sc + JK_NA_OFF_QOFF);
-    // host bins and the segment descriptor are staged by the copy engine from
-    // pageable memory: the copies return once the host data has been taken
+    // the host bins are staged by the copy engine from pageable memory: the
+    // copies return once the host data has been taken
     cudaError_t e = cudaMemcpyAsync(d_bins_ij, bins_locs_ij, sizeof(int) * (nbins + 1), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(d_bins_kl, bins_locs_kl, sizeof(int) * (nbins + 1), cudaMemcpyHostToDevice, st);
     JKSeg seg;
     jk_internal_fill_seg(b, cp_ij, cp_kl, d_qoff, n_ij, dm, n_dm, vj, vk, &seg);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_seg, &seg, sizeof(JKSeg), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return jk_internal_set_err(JK_ERR_CUDA, cudaGetErrorString(e));
     jk_na_qoff_kernel<<<1, 1024, 0, st>>>(d_bins_ij, d_bins_kl, nbins, n_ij, cp_ij == cp_kl, d_qoff, d_task0);
     e = cudaGetLastError();
     if (e != cudaSuccess) return jk_internal_set_err(JK_ERR_CUDA, cudaGetErrorString(e));
     long long max_tasks = cp_ij == cp_kl ? (long long)n_ij * (n_ij + 1) / 2 : (long long)n_ij * n_kl;
-    return jk_internal_launch(b, cp_ij, cp_kl, d_seg, d_task0, max_tasks, stream);
+    return jk_internal_launch(b, cp_ij, cp_kl, seg, d_task0, max_tasks, stream);
 }

@@ -253,7 +253,15 @@ int main(int argc, char **argv) {
     fprintf(fo, "};\nRYS_META double rys_herm_w[%d] = {", nmax * (nmax + 1) / 2);
     for (int n = 1; n <= nmax; n++)
         for (int i = 0; i < n; i++) fprintf(fo, "%s%a", (n == 1 && i == 0) ? "" : ", ", (double)hh[n][i]);
-    fprintf(fo, "};\n#ifdef RYS_WANT_COEF\nstatic const double rys_coef[%d] = {\n", off[nmax + 1]);
+    fprintf(fo, "};\n/* compile-time copies of the per-n sizes */\n#ifdef __CUDACC__\n#define RYS_HD __host__ __device__\n"
+                "#else\n#define RYS_HD\n#endif\nRYS_HD constexpr int rys_nint_c(int n) { return ");
+    for (int n = 1; n <= nmax; n++) fprintf(fo, "n == %d ? %d : ", n, nint[n]);
+    fprintf(fo, "0; }\nRYS_HD constexpr int rys_off_c(int n) { return ");
+    for (int n = 1; n <= nmax; n++) fprintf(fo, "n == %d ? %d : ", n, off[n]);
+    fprintf(fo, "0; }\nRYS_HD constexpr double rys_xmax_c(int n) { return ");
+    for (int n = 1; n <= nmax; n++) fprintf(fo, "n == %d ? %a : ", n, xas[n]);
+    fprintf(fo, "0.; }\n");
+    fprintf(fo, "#ifdef RYS_WANT_COEF\nstatic const double rys_coef[%d] = {\n", off[nmax + 1]);
     for (int n = 1; n <= nmax; n++) {
         size_t cnt = (size_t)nint[n] * 2 * n * NC;
         for (size_t k = 0; k < cnt; k++)

@@ -50,7 +50,8 @@ _SIGNATURES = {
     'jk_rys_roots_host': [ctypes.c_int, ctypes.c_double, ctypes.c_void_p,
                           ctypes.c_void_p],
     'jk_rys_roots_device': [ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
-                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                            ctypes.c_void_p],
     'jk_basis_cq_info': [ctypes.c_void_p, ctypes.c_void_p],
     'jk_last_counts': [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
     'jk_fma_peak': [ctypes.c_int, ctypes.c_void_p],

@@ -118,9 +118,12 @@ int jk_get_jk(jk_basis_t *basis, const double *coeff, int nao0, const double *dm
  * host (for checking the tables).  Returns JK_ERR_ARG for n outside 1..11. */
 int jk_rys_roots_host(int n, double x, double *s, double *w);
 
-/* The same tables evaluated by a device kernel: x, s, w are device arrays
- * (count, count*n, count*n).  For checking the device copy of the tables. */
-int jk_rys_roots_device(int n, const double *x, int count, double *s, double *w, void *stream);
+/* The same tables evaluated by a device kernel through the paths the J/K
+ * kernels use (mode 0: all roots from the shared-memory copy, 1: one root at
+ * a time from it, 2: one root from the global copy; n = 1 is evaluated from
+ * the Boys function in every mode).  x, s, w are device arrays (count,
+ * count*n, count*n).  For checking the device evaluation. */
+int jk_rys_roots_device(int n, const double *x, int count, double *s, double *w, int mode, void *stream);
 
 /* Per class quartet (8 ints each): cp_ij, cp_kl, li, lj, lk, ll, nprim_ij,
  * nprim_kl.  No reference counterpart: introspection for the cost model. */

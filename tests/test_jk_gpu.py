@@ -82,22 +82,27 @@ def test_pairs_and_qcond_vs_oracle():
 
 
 def test_device_rys_tables_match_host():
+    """Device evaluation (every kernel path) against the host evaluation of
+    the tables; n = 1 is the Boys function on the device, the table on the
+    host, so that case checks the two against each other."""
     import torch
     from byteqc_b200.cuobc import lib as jklib
     lib = jklib.load_library()
     rng = np.random.default_rng(1)
-    xs = np.concatenate([[0., 1e-13, 1.0, 2.0, 41.9, 42.0, 97.9, 200., 1e5],
-                         rng.uniform(0, 120, 200)])
+    xs = np.concatenate([[0., 1e-13, 0.5, 0.7499, 0.75, 1.0, 2.0, 41.9, 42.0,
+                          97.9, 200., 1e5], rng.uniform(0, 120, 200)])
     dx = torch.as_tensor(xs, device='cuda')
     for n in range(1, 12):
-        ds = torch.zeros(len(xs) * n, dtype=torch.float64, device='cuda')
-        dw = torch.zeros_like(ds)
-        assert lib.jk_rys_roots_device(n, dx.data_ptr(), len(xs), ds.data_ptr(),
-                                       dw.data_ptr(), None) == 0
-        s = ds.cpu().numpy().reshape(-1, n)
-        w = dw.cpu().numpy().reshape(-1, n)
-        for i, x in enumerate(xs):
-            hs, hw = np.zeros(n), np.zeros(n)
-            lib.jk_rys_roots_host(n, x, hs.ctypes.data, hw.ctypes.data)
-            np.testing.assert_allclose(s[i], hs, rtol=1e-14, atol=1e-300)
-            np.testing.assert_allclose(w[i], hw, rtol=1e-14, atol=1e-300)
+        for mode in range(3):
+            ds = torch.zeros(len(xs) * n, dtype=torch.float64, device='cuda')
+            dw = torch.zeros_like(ds)
+            assert lib.jk_rys_roots_device(n, dx.data_ptr(), len(xs),
+                                           ds.data_ptr(), dw.data_ptr(), mode,
+                                           None) == 0
+            s = ds.cpu().numpy().reshape(-1, n)
+            w = dw.cpu().numpy().reshape(-1, n)
+            for i, x in enumerate(xs):
+                hs, hw = np.zeros(n), np.zeros(n)
+                lib.jk_rys_roots_host(n, x, hs.ctypes.data, hw.ctypes.data)
+                np.testing.assert_allclose(s[i], hs, rtol=1e-14, atol=1e-300)
+                np.testing.assert_allclose(w[i], hw, rtol=1e-14, atol=1e-300)
