@@ -283,6 +283,12 @@ def main():
     quartets = int(counts[:ncq].sum())
     flops = sum(int(c) * class_flops(*(int(v) for v in cq[i, 2:8]))
                 for i, c in enumerate(counts[:ncq]) if c)
+    # one FP64 atomic per element of the six J/K blocks of every quartet
+    atomics = 0
+    for i, c in enumerate(counts[:ncq]):
+        fi, fj, fk, fl = (ncart(int(v)) for v in cq[i, 2:6])
+        atomics += int(c) * (fi * fj + fk * fl + fi * fk + fi * fl + fj * fk
+                             + fj * fl)
     peak = ctypes.c_double()
     lib.jk_fma_peak(0, ctypes.byref(peak))
     achieved = flops / (ms_kern * 1e-3) / 1e12
@@ -309,6 +315,7 @@ def main():
         'quartets_per_build': quartets,
         'quartets_per_s': world * quartets / (ms_step * 1e-3),
         'kernel_ms_per_build': ms_kern,
+        'atomics_per_build': atomics,
         'setup_s': setup_s,
         # dm_cond + screen + one launch per class quartet + 2 symmetrize
         'gpu_launches': 4 + ncq,

@@ -48,10 +48,8 @@ struct JKQuartet {
     double norm;
 };
 
-__device__ __forceinline__ JKQuartet jk_decode(const JKSeg& sg, long long local) {
+__device__ __forceinline__ JKQuartet jk_quartet_at(const JKSeg& sg, int row, int col) {
     JKQuartet q;
-    int row = jk_find_row(sg.qoff, sg.n_ij, local);
-    int col = (int)(local - __ldg(sg.qoff + row));
     int bij = sg.pair_ij0 + row, bkl = sg.pair_kl0 + col;
     q.ish = __ldg(sg.pair2bra + bij);
     q.jsh = __ldg(sg.pair2ket + bij);
@@ -63,6 +61,28 @@ __device__ __forceinline__ JKQuartet jk_decode(const JKSeg& sg, long long local)
     q.norm = JK_FAC * (bij == bkl ? 0.5 : 1.0);
     return q;
 }
+
+// Walks the tasks t = t0, t0 + step, ... of one segment in increasing order,
+// keeping the (row, row start, row end) of the last task so that each step
+// costs a few comparisons instead of a binary search over the rows.
+struct JKTaskCursor {
+    int row;
+    long long rbeg, rend;
+    __device__ __forceinline__ void init(const JKSeg& sg, long long t) {
+        row = jk_find_row(sg.qoff, sg.n_ij, t);
+        rbeg = __ldg(sg.qoff + row);
+        rend = __ldg(sg.qoff + row + 1);
+    }
+    // column of task t (t not below the previous task)
+    __device__ __forceinline__ int seek(const JKSeg& sg, long long t) {
+        while (t >= rend) {
+            row++;
+            rbeg = rend;
+            rend = __ldg(sg.qoff + row + 1);
+        }
+        return (int)(t - rbeg);
+    }
+};
 
 // prefactors of one primitive quartet
 struct JKPrim {
@@ -249,10 +269,21 @@ __global__ void __launch_bounds__(128, C::MINB) jk_thread_kernel(const __grid_co
     extern __shared__ __align__(16) double jk_tab[];
     rys_table_to_smem<C::NROOTS>(sg.rys, jk_tab);
     __syncthreads();
+    // each warp takes a contiguous chunk of tasks (a multiple of 32); lane i
+    // does tasks i, i+32, ... of it, so a warp covers consecutive kl of a row
     const long long total = task0[1];
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
-        JKQuartet q = jk_decode(sg, t);
+    const int lane = threadIdx.x & 31;
+    const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+    const long long wid = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const long long chunk = (((total + nwarps - 1) / nwarps) + 31) & ~31LL;
+    long long t = wid * chunk + lane;
+    const long long tend = min(total, (wid + 1) * chunk);
+    if (t >= tend) return;
+    JKTaskCursor cur;
+    cur.init(sg, t);
+    for (; t < tend; t += 32) {
+        int col = cur.seek(sg, t);
+        JKQuartet q = jk_quartet_at(sg, cur.row, col);
         jk_thread_quartet<C, R>(sg, q, jk_tab);
     }
 }
@@ -316,15 +347,22 @@ __global__ void jk_team_kernel(const __grid_constant__ JKSeg sg0, const long lon
     __syncthreads();
     const JKSeg& sg = sg0;
     const long long total = task0[1];
-    const long long nteams = (long long)gridDim.x * S::QPB;
     const int nprim_ij = sg.nprim_ij, nprim_kl = sg.nprim_kl;
-    for (long long base = (long long)blockIdx.x * S::QPB; base < total; base += nteams) {
-        const long long t = base + team;
-        const bool active = t < total;
+    // each team takes a contiguous chunk of tasks; every team of the block
+    // runs the same number of iterations (the block synchronises inside)
+    const long long nteams = (long long)gridDim.x * S::QPB;
+    const long long tid = (long long)blockIdx.x * S::QPB + team;
+    const long long chunk = (total + nteams - 1) / nteams;
+    const long long tbeg = tid * chunk, tend = min(total, tbeg + chunk);
+    JKTaskCursor cur;
+    if (tbeg < tend) cur.init(sg, tbeg);
+    for (long long it = 0; it < chunk; it++) {
+        const long long t = tbeg + it;
+        const bool active = t < tend;
         JKQuartet q;
         double ri[3], rj[3], rk[3], rl[3];
         if (active) {
-            q = jk_decode(sg, t);
+            q = jk_quartet_at(sg, cur.row, cur.seek(sg, t));
             load_center(sg, q.ish, ri);
             load_center(sg, q.jsh, rj);
             load_center(sg, q.ksh, rk);
