@@ -227,10 +227,18 @@ struct JKClass {
     static constexpr int GS = (LI + 1) * SI;
     // ownership: P leading centres are owned by a thread of the team; the
     // remaining Cartesian components are accumulated in registers
-    // one thread per quartet when its accumulators and one root's 2D blocks
-    // fit in registers (W doubles), else a team
-    static constexpr int W = NF + 3 * GS;
-    static constexpr int P = (W <= 64) ? 0 : ((NF / NFI <= 64) ? 1 : 2);
+    // One thread per quartet (P = 0) when one root's 2D blocks and the
+    // accumulators of GI bra components fit in registers: in one pass if all
+    // components fit (W <= 64 doubles), else in NPASS <= 4 passes over the
+    // primitives with GI bra components each (<= 80 doubles live).  Larger
+    // classes use a team per quartet (P = 1: owned i; P = 2: owned i and j).
+    static constexpr int EI = NFJ * NFK * NFL;  // components per bra index
+    static constexpr int GI1 = (80 - 3 * GS) / EI;
+    static constexpr int GI = (NF + 3 * GS <= 64) ? NFI : (3 * GS <= 48 && GI1 >= 1 ? GI1 : 0);
+    static constexpr int NPASS = GI ? (NFI + GI - 1) / GI : 0;
+    static constexpr bool THREAD = GI > 0 && NPASS <= 4;
+    static constexpr int W = (THREAD ? (GI < NFI ? GI : NFI) * EI : NF) + 3 * GS;
+    static constexpr int P = THREAD ? 0 : ((NF / NFI <= 64) ? 1 : 2);
     static constexpr int T = P == 0 ? 1 : (P == 1 ? NFI : NFI * NFJ);
     static constexpr int NACC = NF / T;
     // resident 128-thread blocks asked of the register allocator (thread kernel)

@@ -138,19 +138,21 @@ __device__ __forceinline__ void load_center(const JKSeg& sg, int sh, double* r) 
 #define DM(a, b) __ldg(D + (a) + (size_t)nao * (b))
 
 // ===========================================================================
-// P = 0: one thread per quartet
+// P = 0: one thread per quartet.  The Cartesian components are accumulated
+// for bra indices ci in [CI0, CI1) per pass; classes too large for one pass
+// run NPASS passes over the primitive quartets (the 2D blocks are rebuilt
+// per pass, the accumulators of one pass only are live).
 // ===========================================================================
-template <class C, typename R>
-__device__ __forceinline__ void jk_thread_quartet(const JKSeg& sg, const JKQuartet& q, const double* __restrict__ tab) {
+template <class C, typename R, int CI0, int CI1>
+__device__ __forceinline__ void jk_thread_pass(const JKSeg& sg, const JKQuartet& q, const double* __restrict__ tab,
+                                               const double* ri, const double* rj, const double* rk,
+                                               const double* rl) {
     constexpr int NR = C::NROOTS;
-    double ri[3], rj[3], rk[3], rl[3];
-    load_center(sg, q.ish, ri);
-    load_center(sg, q.jsh, rj);
-    load_center(sg, q.ksh, rk);
-    load_center(sg, q.lsh, rl);
-    R acc[C::NF];
+    constexpr int NI = CI1 - CI0;
+    constexpr int NA = NI * C::NFJ * C::NFK * C::NFL;
+    R acc[NA];
 #pragma unroll
-    for (int e = 0; e < C::NF; e++) acc[e] = R(0);
+    for (int e = 0; e < NA; e++) acc[e] = R(0);
     for (int ip = 0; ip < sg.nprim_ij; ip++)
         for (int kp = 0; kp < sg.nprim_kl; kp++) {
             JKPrim p = jk_prim(sg, q.prim_ij + ip, q.prim_kl + kp);
@@ -164,25 +166,25 @@ __device__ __forceinline__ void jk_thread_quartet(const JKSeg& sg, const JKQuart
                 jk_unit<C, R>(p, s, w, 1, q.norm, ri, rj, rk, rl, Iy);
                 jk_unit<C, R>(p, s, w, 2, q.norm, ri, rj, rk, rl, Iz);
 #pragma unroll
-                for (int i = 0; i < C::NFI; i++)
+                for (int i = 0; i < NI; i++)
 #pragma unroll
                     for (int j = 0; j < C::NFJ; j++)
 #pragma unroll
                         for (int k = 0; k < C::NFK; k++)
 #pragma unroll
                             for (int l = 0; l < C::NFL; l++) {
-                                int ox = cart_lx(C::LI, i) * C::SI + cart_lx(C::LJ, j) * C::SJ +
+                                int ox = cart_lx(C::LI, CI0 + i) * C::SI + cart_lx(C::LJ, j) * C::SJ +
                                          cart_lx(C::LK, k) * C::SK + cart_lx(C::LL, l);
-                                int oy = cart_ly(C::LI, i) * C::SI + cart_ly(C::LJ, j) * C::SJ +
+                                int oy = cart_ly(C::LI, CI0 + i) * C::SI + cart_ly(C::LJ, j) * C::SJ +
                                          cart_ly(C::LK, k) * C::SK + cart_ly(C::LL, l);
-                                int oz = cart_lz(C::LI, i) * C::SI + cart_lz(C::LJ, j) * C::SJ +
+                                int oz = cart_lz(C::LI, CI0 + i) * C::SI + cart_lz(C::LJ, j) * C::SJ +
                                          cart_lz(C::LK, k) * C::SK + cart_lz(C::LL, l);
                                 acc[((i * C::NFJ + j) * C::NFK + k) * C::NFL + l] += Ix[ox] * Iy[oy] * Iz[oz];
                             }
             }
         }
     const int nao = sg.nao;
-    const int i0 = __ldg(sg.ao_loc + q.ish), j0 = __ldg(sg.ao_loc + q.jsh);
+    const int i0 = __ldg(sg.ao_loc + q.ish) + CI0, j0 = __ldg(sg.ao_loc + q.jsh);
     const int k0 = __ldg(sg.ao_loc + q.ksh), l0 = __ldg(sg.ao_loc + q.lsh);
 #define ACC(i, j, k, l) ((double)acc[(((i) * C::NFJ + (j)) * C::NFK + (k)) * C::NFL + (l)])
     for (int idm = 0; idm < sg.n_dm; idm++) {
@@ -190,7 +192,7 @@ __device__ __forceinline__ void jk_thread_quartet(const JKSeg& sg, const JKQuart
         if (sg.vj) {
             double* V = sg.vj + (size_t)idm * nao * nao;
 #pragma unroll
-            for (int i = 0; i < C::NFI; i++)
+            for (int i = 0; i < NI; i++)
 #pragma unroll
                 for (int j = 0; j < C::NFJ; j++) {
                     double v = 0;
@@ -206,7 +208,7 @@ __device__ __forceinline__ void jk_thread_quartet(const JKSeg& sg, const JKQuart
                 for (int l = 0; l < C::NFL; l++) {
                     double v = 0;
 #pragma unroll
-                    for (int i = 0; i < C::NFI; i++)
+                    for (int i = 0; i < NI; i++)
 #pragma unroll
                         for (int j = 0; j < C::NFJ; j++) v += ACC(i, j, k, l) * DM(i0 + i, j0 + j);
                     atomicAdd(V + (k0 + k) + (size_t)nao * (l0 + l), v);
@@ -215,7 +217,7 @@ __device__ __forceinline__ void jk_thread_quartet(const JKSeg& sg, const JKQuart
         if (sg.vk) {
             double* V = sg.vk + (size_t)idm * nao * nao;
 #pragma unroll
-            for (int i = 0; i < C::NFI; i++)
+            for (int i = 0; i < NI; i++)
 #pragma unroll
                 for (int k = 0; k < C::NFK; k++) {
                     double v = 0;
@@ -226,7 +228,7 @@ __device__ __forceinline__ void jk_thread_quartet(const JKSeg& sg, const JKQuart
                     atomicAdd(V + (i0 + i) + (size_t)nao * (k0 + k), v);
                 }
 #pragma unroll
-            for (int i = 0; i < C::NFI; i++)
+            for (int i = 0; i < NI; i++)
 #pragma unroll
                 for (int l = 0; l < C::NFL; l++) {
                     double v = 0;
@@ -242,7 +244,7 @@ __device__ __forceinline__ void jk_thread_quartet(const JKSeg& sg, const JKQuart
                 for (int k = 0; k < C::NFK; k++) {
                     double v = 0;
 #pragma unroll
-                    for (int i = 0; i < C::NFI; i++)
+                    for (int i = 0; i < NI; i++)
 #pragma unroll
                         for (int l = 0; l < C::NFL; l++) v += ACC(i, j, k, l) * DM(i0 + i, l0 + l);
                     atomicAdd(V + (j0 + j) + (size_t)nao * (k0 + k), v);
@@ -253,7 +255,7 @@ __device__ __forceinline__ void jk_thread_quartet(const JKSeg& sg, const JKQuart
                 for (int l = 0; l < C::NFL; l++) {
                     double v = 0;
 #pragma unroll
-                    for (int i = 0; i < C::NFI; i++)
+                    for (int i = 0; i < NI; i++)
 #pragma unroll
                         for (int k = 0; k < C::NFK; k++) v += ACC(i, j, k, l) * DM(i0 + i, k0 + k);
                     atomicAdd(V + (j0 + j) + (size_t)nao * (l0 + l), v);
@@ -261,6 +263,28 @@ __device__ __forceinline__ void jk_thread_quartet(const JKSeg& sg, const JKQuart
         }
     }
 #undef ACC
+}
+
+template <class C, typename R, int PASS>
+__device__ __forceinline__ void jk_thread_passes(const JKSeg& sg, const JKQuartet& q, const double* __restrict__ tab,
+                                                 const double* ri, const double* rj, const double* rk,
+                                                 const double* rl) {
+    constexpr int CI0 = PASS * C::GI;
+    if constexpr (CI0 < C::NFI) {
+        constexpr int CI1 = CI0 + C::GI < C::NFI ? CI0 + C::GI : C::NFI;
+        jk_thread_pass<C, R, CI0, CI1>(sg, q, tab, ri, rj, rk, rl);
+        jk_thread_passes<C, R, PASS + 1>(sg, q, tab, ri, rj, rk, rl);
+    }
+}
+
+template <class C, typename R>
+__device__ __forceinline__ void jk_thread_quartet(const JKSeg& sg, const JKQuartet& q, const double* __restrict__ tab) {
+    double ri[3], rj[3], rk[3], rl[3];
+    load_center(sg, q.ish, ri);
+    load_center(sg, q.jsh, rj);
+    load_center(sg, q.ksh, rk);
+    load_center(sg, q.lsh, rl);
+    jk_thread_passes<C, R, 0>(sg, q, tab, ri, rj, rk, rl);
 }
 
 template <class C, typename R>
