@@ -324,16 +324,34 @@ struct JKTeamShape {
     static constexpr int BWORDS_RAW = C::NFI * C::NFJ + C::NFK * C::NFL + C::NFI * C::NFK + C::NFI * C::NFL +
                                       C::NFJ * C::NFK + C::NFJ * C::NFL;  // digestion buffers
     static constexpr int BWORDS = BWORDS_RAW | 1;
-    static constexpr int TAB = RysS<C::NROOTS>::WORDS;  // Rys table (doubles), first in shared memory
+    // per-thread partial J/K blocks of the digestion (reuse the 2D-block space)
+    static constexpr int NKET = C::NFK * C::NFL;
+    static constexpr int PSTRIDE = C::P == 1 ? NKET + C::NFJ * C::NFK + C::NFJ * C::NFL
+                                             : NKET + 2 * C::NFK + 2 * C::NFL;  // doubles per thread
+    static constexpr int PWORDS = C::T * PSTRIDE;
+    // the Rys table goes to shared memory for up to 4 roots; beyond that the
+    // units read the global copy (it would cost 37-60 KB per block)
+    static constexpr bool SMEM_TAB = C::NROOTS <= 4;
+    static constexpr int TAB = SMEM_TAB ? RysS<C::NROOTS>::WORDS : 0;  // doubles, first in shared memory
     static constexpr int OFF_JIJ = 0, OFF_JKL = OFF_JIJ + C::NFI * C::NFJ, OFF_KIK = OFF_JKL + C::NFK * C::NFL,
                          OFF_KIL = OFF_KIK + C::NFI * C::NFK, OFF_KJK = OFF_KIL + C::NFI * C::NFL,
                          OFF_KJL = OFF_KJK + C::NFJ * C::NFK;
 };
 
+// bytes per team of the region shared by the 2D blocks and the digestion
+// partials (an odd number of doubles)
+template <class C, typename R>
+__host__ __device__ constexpr size_t jk_team_region() {
+    using S = JKTeamShape<C>;
+    size_t g = (size_t)S::GWORDS * sizeof(R), p = (size_t)S::PWORDS * sizeof(double);
+    size_t words = ((g > p ? g : p) + 7) / 8;
+    return (words | 1) * 8;
+}
+
 template <class C, typename R>
 __host__ __device__ constexpr size_t jk_team_gbytes() {
     using S = JKTeamShape<C>;
-    return ((size_t)S::QPB * S::GWORDS * sizeof(R) + 15) & ~(size_t)15;
+    return ((size_t)S::QPB * jk_team_region<C, R>() + 15) & ~(size_t)15;
 }
 
 template <class C, typename R>
@@ -350,9 +368,10 @@ __global__ void jk_team_kernel(const __grid_constant__ JKSeg sg0, const long lon
     const int team = threadIdx.x / T, lane = threadIdx.x - team * T;
     double* tab = reinterpret_cast<double*>(jk_smem);
     unsigned char* gbase = jk_smem + (size_t)S::TAB * sizeof(double);
-    R* g = reinterpret_cast<R*>(gbase) + (size_t)team * S::GWORDS;
+    R* g = reinterpret_cast<R*>(gbase + (size_t)team * jk_team_region<C, R>());
+    double* part = reinterpret_cast<double*>(g);  // digestion partials reuse the 2D-block space
     double* buf = reinterpret_cast<double*>(gbase + jk_team_gbytes<C, R>()) + (size_t)team * S::BWORDS;
-    rys_table_to_smem<NR>(sg0.rys, tab);
+    if (S::SMEM_TAB) rys_table_to_smem<NR>(sg0.rys, tab);
 
     // owned Cartesian indices
     int ci = 0, cj = 0;
@@ -402,7 +421,8 @@ __global__ void jk_team_kernel(const __grid_constant__ JKSeg sg0, const long lon
                     for (int u = lane; u < 3 * NR; u += T) {
                         int r = u / 3, d = u - 3 * r;
                         double s, w;
-                        rys_root_one<NR>(tab, p.x, r, s, w);
+                        if (S::SMEM_TAB) rys_root_one<NR>(tab, p.x, r, s, w);
+                        else rys_root<NR>(sg.rys, p.x, r, s, w);
                         jk_unit<C, R>(p, s, w, d, q.norm, ri, rj, rk, rl, g + u * C::GS);
                     }
                 }
@@ -443,10 +463,13 @@ __global__ void jk_team_kernel(const __grid_constant__ JKSeg sg0, const long lon
             }
 
         // ---- digestion ----
+        // Outputs a thread owns completely go to buf; the others are written as
+        // per-thread partials (no shared atomics), summed by the team after a
+        // barrier, then every element is flushed with one global atomic.
         const int n_dm = sg.n_dm;
         for (int idm = 0; idm < n_dm; idm++) {
-            for (int e = lane; e < S::BWORDS; e += T) buf[e] = 0.;
-            __syncthreads();
+            // every element of buf is written below before it is flushed
+            double* mine = part + (size_t)lane * S::PSTRIDE;
             if (active) {
                 const int nao = sg.nao;
                 const int i0 = __ldg(sg.ao_loc + q.ish), j0 = __ldg(sg.ao_loc + q.jsh);
@@ -455,6 +478,9 @@ __global__ void jk_team_kernel(const __grid_constant__ JKSeg sg0, const long lon
                 if (C::P == 1) {
 #define A1(j, k, l) ((double)acc[((j) * C::NFK + (k)) * C::NFL + (l)])
                     const int I = i0 + ci;
+                    double* pjkl = mine;
+                    double* pkjk = mine + S::NKET;
+                    double* pkjl = pkjk + C::NFJ * C::NFK;
                     if (sg.vj) {
 #pragma unroll
                         for (int j = 0; j < C::NFJ; j++) {  // J_ij: complete in-thread
@@ -466,13 +492,13 @@ __global__ void jk_team_kernel(const __grid_constant__ JKSeg sg0, const long lon
                             buf[S::OFF_JIJ + ci * C::NFJ + j] = v;
                         }
 #pragma unroll
-                        for (int k = 0; k < C::NFK; k++)  // J_kl: reduce over i
+                        for (int k = 0; k < C::NFK; k++)  // J_kl: partial over i
 #pragma unroll
                             for (int l = 0; l < C::NFL; l++) {
                                 double v = 0;
 #pragma unroll
                                 for (int j = 0; j < C::NFJ; j++) v += A1(j, k, l) * DM(I, j0 + j);
-                                atomicAdd(buf + S::OFF_JKL + k * C::NFL + l, v);
+                                pjkl[k * C::NFL + l] = v;
                             }
                     }
                     if (sg.vk) {
@@ -497,26 +523,31 @@ __global__ void jk_team_kernel(const __grid_constant__ JKSeg sg0, const long lon
 #pragma unroll
                         for (int j = 0; j < C::NFJ; j++)
 #pragma unroll
-                            for (int k = 0; k < C::NFK; k++) {  // K_jk: reduce over i
+                            for (int k = 0; k < C::NFK; k++) {  // K_jk: partial over i
                                 double v = 0;
 #pragma unroll
                                 for (int l = 0; l < C::NFL; l++) v += A1(j, k, l) * DM(I, l0 + l);
-                                atomicAdd(buf + S::OFF_KJK + j * C::NFK + k, v);
+                                pkjk[j * C::NFK + k] = v;
                             }
 #pragma unroll
                         for (int j = 0; j < C::NFJ; j++)
 #pragma unroll
-                            for (int l = 0; l < C::NFL; l++) {  // K_jl: reduce over i
+                            for (int l = 0; l < C::NFL; l++) {  // K_jl: partial over i
                                 double v = 0;
 #pragma unroll
                                 for (int k = 0; k < C::NFK; k++) v += A1(j, k, l) * DM(I, k0 + k);
-                                atomicAdd(buf + S::OFF_KJL + j * C::NFL + l, v);
+                                pkjl[j * C::NFL + l] = v;
                             }
                     }
 #undef A1
                 } else {
 #define A2(k, l) ((double)acc[(k) * C::NFL + (l)])
                     const int I = i0 + ci, J = j0 + cj;
+                    double* pjkl = mine;
+                    double* pkik = mine + S::NKET;
+                    double* pkjk = pkik + C::NFK;
+                    double* pkil = pkjk + C::NFK;
+                    double* pkjl = pkil + C::NFL;
                     if (sg.vj) {
                         double v = 0;  // J_ij: complete
 #pragma unroll
@@ -528,7 +559,7 @@ __global__ void jk_team_kernel(const __grid_constant__ JKSeg sg0, const long lon
 #pragma unroll
                         for (int k = 0; k < C::NFK; k++)
 #pragma unroll
-                            for (int l = 0; l < C::NFL; l++) atomicAdd(buf + S::OFF_JKL + k * C::NFL + l, A2(k, l) * dij);
+                            for (int l = 0; l < C::NFL; l++) pjkl[k * C::NFL + l] = A2(k, l) * dij;
                     }
                     if (sg.vk) {
 #pragma unroll
@@ -539,8 +570,8 @@ __global__ void jk_team_kernel(const __grid_constant__ JKSeg sg0, const long lon
                                 vik += A2(k, l) * DM(J, l0 + l);
                                 vjk += A2(k, l) * DM(I, l0 + l);
                             }
-                            atomicAdd(buf + S::OFF_KIK + ci * C::NFK + k, vik);
-                            atomicAdd(buf + S::OFF_KJK + cj * C::NFK + k, vjk);
+                            pkik[k] = vik;
+                            pkjk[k] = vjk;
                         }
 #pragma unroll
                         for (int l = 0; l < C::NFL; l++) {  // K_il (over j) and K_jl (over i)
@@ -550,11 +581,66 @@ __global__ void jk_team_kernel(const __grid_constant__ JKSeg sg0, const long lon
                                 vil += A2(k, l) * DM(J, k0 + k);
                                 vjl += A2(k, l) * DM(I, k0 + k);
                             }
-                            atomicAdd(buf + S::OFF_KIL + ci * C::NFL + l, vil);
-                            atomicAdd(buf + S::OFF_KJL + cj * C::NFL + l, vjl);
+                            pkil[l] = vil;
+                            pkjl[l] = vjl;
                         }
                     }
 #undef A2
+                }
+            }
+            __syncthreads();
+            if (active) {  // sum the partials of the team into buf
+                const double* P0 = part;
+                const bool dj = sg.vj != nullptr, dk = sg.vk != nullptr;
+                if (dj)
+                    for (int b = lane; b < S::NKET; b += T) {
+                        double v = 0;
+                        for (int t2 = 0; t2 < T; t2++) v += P0[(size_t)t2 * S::PSTRIDE + b];
+                        buf[S::OFF_JKL + b] = v;
+                    }
+                if (dk && C::P == 1) {
+                    for (int e = lane; e < C::NFJ * C::NFK; e += T) {
+                        double v = 0;
+                        for (int t2 = 0; t2 < T; t2++) v += P0[(size_t)t2 * S::PSTRIDE + S::NKET + e];
+                        buf[S::OFF_KJK + e] = v;
+                    }
+                    for (int e = lane; e < C::NFJ * C::NFL; e += T) {
+                        double v = 0;
+                        for (int t2 = 0; t2 < T; t2++)
+                            v += P0[(size_t)t2 * S::PSTRIDE + S::NKET + C::NFJ * C::NFK + e];
+                        buf[S::OFF_KJL + e] = v;
+                    }
+                }
+                if (dk && C::P == 2) {
+                    // K_ik[i][k] = sum_j, K_jk[j][k] = sum_i, K_il, K_jl likewise
+                    for (int e = lane; e < C::NFI * C::NFK; e += T) {
+                        int i = e / C::NFK, k = e - i * C::NFK;
+                        double v = 0;
+                        for (int j = 0; j < C::NFJ; j++)
+                            v += P0[(size_t)(i * C::NFJ + j) * S::PSTRIDE + S::NKET + k];
+                        buf[S::OFF_KIK + e] = v;
+                    }
+                    for (int e = lane; e < C::NFJ * C::NFK; e += T) {
+                        int j = e / C::NFK, k = e - j * C::NFK;
+                        double v = 0;
+                        for (int i = 0; i < C::NFI; i++)
+                            v += P0[(size_t)(i * C::NFJ + j) * S::PSTRIDE + S::NKET + C::NFK + k];
+                        buf[S::OFF_KJK + e] = v;
+                    }
+                    for (int e = lane; e < C::NFI * C::NFL; e += T) {
+                        int i = e / C::NFL, l = e - i * C::NFL;
+                        double v = 0;
+                        for (int j = 0; j < C::NFJ; j++)
+                            v += P0[(size_t)(i * C::NFJ + j) * S::PSTRIDE + S::NKET + 2 * C::NFK + l];
+                        buf[S::OFF_KIL + e] = v;
+                    }
+                    for (int e = lane; e < C::NFJ * C::NFL; e += T) {
+                        int j = e / C::NFL, l = e - j * C::NFL;
+                        double v = 0;
+                        for (int i = 0; i < C::NFI; i++)
+                            v += P0[(size_t)(i * C::NFJ + j) * S::PSTRIDE + S::NKET + 2 * C::NFK + C::NFL + l];
+                        buf[S::OFF_KJL + e] = v;
+                    }
                 }
             }
             __syncthreads();
@@ -563,7 +649,7 @@ __global__ void jk_team_kernel(const __grid_constant__ JKSeg sg0, const long lon
                 const int i0 = __ldg(sg.ao_loc + q.ish), j0 = __ldg(sg.ao_loc + q.jsh);
                 const int k0 = __ldg(sg.ao_loc + q.ksh), l0 = __ldg(sg.ao_loc + q.lsh);
                 const size_t moff = (size_t)idm * nao * nao;
-                for (int e = lane; e < S::BWORDS; e += T) {
+                for (int e = lane; e < S::BWORDS_RAW; e += T) {  // not the padding word
                     double v = buf[e];
                     double* V;
                     int a, b;
