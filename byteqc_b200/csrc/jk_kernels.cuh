@@ -186,6 +186,14 @@ __device__ __forceinline__ void jk_thread_pass(const JKSeg& sg, const JKQuartet&
     const int nao = sg.nao;
     const int i0 = __ldg(sg.ao_loc + q.ish) + CI0, j0 = __ldg(sg.ao_loc + q.jsh);
     const int k0 = __ldg(sg.ao_loc + q.ksh), l0 = __ldg(sg.ao_loc + q.lsh);
+    // the lanes of a warp usually share the ij pair (consecutive kl of one
+    // row): then the J_ij block is summed over the warp before its atomics
+    const unsigned am = __activemask();
+    bool wsame = false;
+    if (am == 0xffffffffu) {
+        int i_0 = __shfl_sync(am, q.ish, 0), j_0 = __shfl_sync(am, q.jsh, 0);
+        wsame = __all_sync(am, q.ish == i_0 && q.jsh == j_0);
+    }
 #define ACC(i, j, k, l) ((double)acc[(((i) * C::NFJ + (j)) * C::NFK + (k)) * C::NFL + (l)])
     for (int idm = 0; idm < sg.n_dm; idm++) {
         const double* D = sg.dm + (size_t)idm * nao * nao;
@@ -200,7 +208,13 @@ __device__ __forceinline__ void jk_thread_pass(const JKSeg& sg, const JKQuartet&
                     for (int k = 0; k < C::NFK; k++)
 #pragma unroll
                         for (int l = 0; l < C::NFL; l++) v += ACC(i, j, k, l) * DM(k0 + k, l0 + l);
-                    atomicAdd(V + (i0 + i) + (size_t)nao * (j0 + j), v);
+                    if (wsame) {
+#pragma unroll
+                        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                        if ((threadIdx.x & 31) == 0) atomicAdd(V + (i0 + i) + (size_t)nao * (j0 + j), v);
+                    } else {
+                        atomicAdd(V + (i0 + i) + (size_t)nao * (j0 + j), v);
+                    }
                 }
 #pragma unroll
             for (int k = 0; k < C::NFK; k++)
