@@ -184,6 +184,9 @@ def main():
     ap.add_argument('--workload', default='h2o32-tzvp', choices=sorted(WORKLOADS))
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--ref-sample-s', type=float, default=12.0)
+    ap.add_argument('--fp32-cutoff', type=float, default=1e-6,
+                    help='also time the mixed-precision build at this cutoff '
+                         '(0: skip)')
     args = ap.parse_args()
     if args.impl == 'reference':
         return run_reference(args)
@@ -267,10 +270,23 @@ def main():
     def step_e2e():
         hf.get_jk(mol, dm, vhfopt=opt)
     ms_e2e = timed(step_e2e, max(2, args.steps // 2))
+    # mixed precision: same build with FP32 recursion below fp32_cutoff
+    ms_mixed = None
+    mixed_err = None
+    if args.fp32_cutoff > 0:
+        ref_j, ref_k = d_vj.clone(), d_vk.clone()
+        opts.fp32_cutoff = args.fp32_cutoff
+        for _ in range(2):
+            step_device()
+        ms_mixed = timed(step_device, args.steps)
+        mixed_err = max((d_vj - ref_j).abs().max().item(),
+                        (d_vk - ref_k).abs().max().item())
+        opts.fp32_cutoff = 0.
     if dist:
-        t = torch.tensor([ms_step, ms_kern, ms_e2e], device='cuda')
+        t = torch.tensor([ms_step, ms_kern, ms_e2e, ms_mixed or 0.], device='cuda')
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_step, ms_kern, ms_e2e = t.tolist()
+        ms_step, ms_kern, ms_e2e, mm = t.tolist()
+        ms_mixed = mm if ms_mixed is not None else None
 
     # quartet counts and the FLOP model
     info = np.zeros(7, dtype=np.int32)
@@ -278,8 +294,9 @@ def main():
     ncq = int(info[6])
     cq = np.zeros((max(ncq, 1), 8), dtype=np.int32)
     lib.jk_basis_cq_info(opt.handle, cq.ctypes.data)
-    counts = np.zeros(max(ncq, 1), dtype=np.int64)
-    lib.jk_last_counts(opt.handle, counts.ctypes.data, sptr)
+    counts2 = np.zeros(2 * max(ncq, 1), dtype=np.int64)
+    lib.jk_last_counts(opt.handle, counts2.ctypes.data, sptr)
+    counts = counts2[:ncq] + counts2[ncq:2 * ncq]
     quartets = int(counts[:ncq].sum())
     flops = sum(int(c) * class_flops(*(int(v) for v in cq[i, 2:8]))
                 for i, c in enumerate(counts[:ncq]) if c)
@@ -330,6 +347,12 @@ def main():
                 'd2h_bytes_per_step': int(2 * dm.nbytes)},
         'clocks': clk.summary(),
     }
+    if ms_mixed is not None:
+        line['mixed'] = {'fp32_cutoff': args.fp32_cutoff,
+                         'value': world * 1e3 / ms_mixed, 'unit': 'builds/s',
+                         'ms_per_step': ms_mixed,
+                         'speedup_vs_fp64': ms_step / ms_mixed,
+                         'max_abs_err_jk': mixed_err}
     if world == 1 and not args.no_cpu_baseline:
         v, inf = cpu_baseline(mol, dm)
         line['cpu_baseline'] = {

@@ -318,6 +318,7 @@ __device__ __forceinline__ void rys_2d(R seed, R c00, R c0p, R b10, R b01, R b00
 struct JKSeg {
     const double* rys;      // Rys coefficient table (device)
     const long long* qoff;  // n_ij + 1 entries (device)
+    const int* kl_base;     // first kl column of each row (FP32 part of the mixed mode), or null
     int n_ij;
     int pair_ij0, pair_kl0;  // first pair of each class in the pair arrays
     int prim_ij0, prim_kl0;  // first primitive pair of each class

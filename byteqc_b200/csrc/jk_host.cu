@@ -193,20 +193,70 @@ struct JKScreenCQ {
     long long qoff_off;
 };
 
-// One block per class quartet.  Reproduces the reference's screening
-// decision per contracted quartet (cuobc/scf/hf.py:136-145, 567-578 and
-// cuobc/lib/gvhf/nr_jk_driver.cu:252-280):
+// Block-wide inclusive scan of two counts (256 threads), with running carries.
+__device__ __forceinline__ void jk_block_scan2(long long a, long long b, long long& ia, long long& ib,
+                                               long long* wa, long long* wb, long long& carry_a,
+                                               long long& carry_b) {
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int o = 1; o < 32; o <<= 1) {
+        long long ya = __shfl_up_sync(0xffffffffu, a, o), yb = __shfl_up_sync(0xffffffffu, b, o);
+        if (lane >= o) {
+            a += ya;
+            b += yb;
+        }
+    }
+    if (lane == 31) {
+        wa[warp] = a;
+        wb[warp] = b;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        long long x = (lane < (int)(blockDim.x >> 5)) ? wa[lane] : 0;
+        long long y = (lane < (int)(blockDim.x >> 5)) ? wb[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            long long u = __shfl_up_sync(0xffffffffu, x, o), v = __shfl_up_sync(0xffffffffu, y, o);
+            if (lane >= o) {
+                x += u;
+                y += v;
+            }
+        }
+        wa[lane] = x;
+        wb[lane] = y;
+    }
+    __syncthreads();
+    ia = a + (warp ? wa[warp - 1] : 0) + carry_a;
+    ib = b + (warp ? wb[warp - 1] : 0) + carry_b;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) {
+        carry_a = ia;
+        carry_b = ib;
+    }
+    __syncthreads();
+}
+
+// One block (256 threads) per class quartet.  Reproduces the reference's
+// screening decision per contracted quartet (cuobc/scf/hf.py:136-145,
+// 567-578 and cuobc/lib/gvhf/nr_jk_driver.cu:252-280):
 //   skip the class quartet if prescreen and max(dm_cond over its 6 group
 //   pairs) < tol; else with scale = nbins / log(min(tol/sub, 0.1)) and
 //   s = floor(scale * log_q), keep (ij, kl) iff s_ij + s_kl < nbins (and
 //   kl <= ij inside a diagonal class quartet).
 // Because log_q is sorted descending inside a class, the kept kl of a row
 // form a prefix; its length is found by binary search and prefix-summed.
+// Mixed precision (fp32_cutoff > 0): the kept prefix of a row splits again
+// at the bound q_ij q_kl sub = fp32_cutoff (unclipped log q); the leading
+// part (larger bounds) runs in FP64, the tail in FP32.  qoff counts the FP64
+// part, qoff32 the FP32 part, whose first column per row is klb[ij].
 __global__ void jk_screen_kernel(const JKScreenCQ* __restrict__ cqs, const double* __restrict__ log_q,
-                                 const double* __restrict__ dm_cond, int ngroups, double tol, int nbins,
-                                 int prescreen, long long* __restrict__ qoff_all, long long* __restrict__ task0_all) {
+                                 const double* __restrict__ log_q_raw, const double* __restrict__ dm_cond,
+                                 int ngroups, double tol, int nbins, int prescreen, double fp32_cutoff,
+                                 long long* __restrict__ qoff_all, long long* __restrict__ task0_all,
+                                 long long* __restrict__ qoff32_all, long long* __restrict__ task032_all,
+                                 int* __restrict__ klb_all) {
     const JKScreenCQ cq = cqs[blockIdx.x];
     long long* qoff = qoff_all + cq.qoff_off;
+    long long* qoff32 = qoff32_all + cq.qoff_off;
+    int* klb = klb_all + cq.qoff_off;
     const double* c = dm_cond;
     double sub = fmax(fmax(fmax(c[cq.gi * ngroups + cq.gj], c[cq.gk * ngroups + cq.gl]),
                            fmax(c[cq.gi * ngroups + cq.gk], c[cq.gj * ngroups + cq.gk])),
@@ -214,19 +264,24 @@ __global__ void jk_screen_kernel(const JKScreenCQ* __restrict__ cqs, const doubl
     bool skip = prescreen && sub < tol;
     double cutoff = tol / sub;
     double scale = nbins / log(fmin(cutoff, 0.1));
+    const bool mixed = fp32_cutoff > 0;
+    const double log_thr = mixed ? log(fp32_cutoff / sub) : 0.;  // q_ij q_kl >= fp32_cutoff / sub
     const double* lq_ij = log_q + cq.pair_ij0;
     const double* lq_kl = log_q + cq.pair_kl0;
+    const double* rq_ij = log_q_raw + cq.pair_ij0;
+    const double* rq_kl = log_q_raw + cq.pair_kl0;
     bool diag = cq.cp_ij == cq.cp_kl;
-    __shared__ long long carry;
-    __shared__ long long wsum[32];
+    __shared__ long long carry, carry32;
+    __shared__ long long wsum[32], wsum32[32];
     if (threadIdx.x == 0) {
-        carry = 0;
+        carry = carry32 = 0;
         qoff[0] = 0;
+        qoff32[0] = 0;
     }
     __syncthreads();
     for (int base = 0; base < cq.n_ij; base += blockDim.x) {
         int ij = base + threadIdx.x;
-        long long cnt = 0;
+        long long cnt = 0, c64 = 0;
         if (!skip && ij < cq.n_ij) {
             int sij = (int)floor(scale * lq_ij[ij]);
             if (sij < nbins) {
@@ -241,33 +296,30 @@ __global__ void jk_screen_kernel(const JKScreenCQ* __restrict__ cqs, const doubl
                 if (diag && cnt > ij + 1) cnt = ij + 1;
             }
         }
-        // block inclusive scan of cnt
-        long long v = cnt;
-        int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        for (int o = 1; o < 32; o <<= 1) {
-            long long y = __shfl_up_sync(0xffffffffu, v, o);
-            if (lane >= o) v += y;
-        }
-        if (lane == 31) wsum[warp] = v;
-        __syncthreads();
-        if (warp == 0) {
-            long long w = (lane < (int)(blockDim.x >> 5)) ? wsum[lane] : 0;
-            for (int o = 1; o < 32; o <<= 1) {
-                long long y = __shfl_up_sync(0xffffffffu, w, o);
-                if (lane >= o) w += y;
+        c64 = cnt;
+        if (mixed && cnt > 0) {
+            // kl with rq_ij + rq_kl >= log_thr (non-increasing in kl)
+            double need = log_thr - rq_ij[ij];
+            int lo = 0, hi = (int)cnt;
+            while (lo < hi) {
+                int mid = (lo + hi) >> 1;
+                if (rq_kl[mid] >= need) lo = mid + 1; else hi = mid;
             }
-            wsum[lane] = w;
+            c64 = lo;
         }
-        __syncthreads();
-        long long incl = v + (warp ? wsum[warp - 1] : 0) + carry;
-        if (ij < cq.n_ij) qoff[ij + 1] = incl;
-        __syncthreads();
-        if (threadIdx.x == blockDim.x - 1) carry = incl;
-        __syncthreads();
+        if (ij < cq.n_ij) klb[ij] = (int)c64;
+        long long i64, i32;
+        jk_block_scan2(c64, cnt - c64, i64, i32, wsum, wsum32, carry, carry32);
+        if (ij < cq.n_ij) {
+            qoff[ij + 1] = i64;
+            qoff32[ij + 1] = i32;
+        }
     }
     if (threadIdx.x == 0) {
         task0_all[2 * blockIdx.x] = 0;
         task0_all[2 * blockIdx.x + 1] = carry;
+        task032_all[2 * blockIdx.x] = 0;
+        task032_all[2 * blockIdx.x + 1] = carry32;
     }
 }
 
@@ -295,7 +347,7 @@ struct jk_basis {
     double diag_fac = 0.5, cutoff = 1e-13;
     std::vector<int> h_ao_loc, h_group_off, h_group_l, h_group_nprim;
     std::vector<int> h_cls_gi, h_cls_gj, h_pair_locs, h_prim_locs, h_pair2bra, h_pair2ket;
-    std::vector<double> h_log_q, h_qcond;
+    std::vector<double> h_log_q, h_log_q_raw, h_qcond;
     std::vector<JKScreenCQ> h_cq;
     std::vector<long long> h_qoff_off;
     long long qoff_total = 0;
@@ -303,10 +355,12 @@ struct jk_basis {
     int *d_atm = nullptr, *d_bas = nullptr, *d_ao_loc = nullptr, *d_group_ao = nullptr;
     double *d_env = nullptr, *d_bas_x = nullptr, *d_qcond = nullptr;
     int *d_pair2bra = nullptr, *d_pair2ket = nullptr;
-    double *d_log_q = nullptr, *d_prim = nullptr;  // prim: a12|e12|x12|y12|z12
+    double *d_log_q = nullptr, *d_log_q_raw = nullptr, *d_prim = nullptr;  // prim: a12|e12|x12|y12|z12
     long long nprim_total = 0;
     JKScreenCQ* d_cq = nullptr;
     long long *d_qoff = nullptr, *d_task0 = nullptr;
+    long long *d_qoff32 = nullptr, *d_task032 = nullptr;  // FP32 part of the mixed mode
+    int* d_klb = nullptr;
     double* d_dm_cond = nullptr;
     // reference-compatible single class-pair path
     long long* d_qoff1 = nullptr;
@@ -332,6 +386,10 @@ static void free_basis(jk_basis* b) {
     cudaFree(b->d_pair2bra);
     cudaFree(b->d_pair2ket);
     cudaFree(b->d_log_q);
+    cudaFree(b->d_log_q_raw);
+    cudaFree(b->d_qoff32);
+    cudaFree(b->d_task032);
+    cudaFree(b->d_klb);
     cudaFree(b->d_prim);
     cudaFree(b->d_cq);
     cudaFree(b->d_qoff);
@@ -490,6 +548,7 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
                 b->h_pair2ket.push_back((int)(e.second % nbas));
                 double lq = log(e.first);
                 b->h_log_q.push_back(lq > 0 ? 0 : lq);
+                b->h_log_q_raw.push_back(lq);
             }
             b->h_cls_gi.push_back(gi);
             b->h_cls_gj.push_back(gj);
@@ -540,6 +599,7 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
     CUDA_TRY(upload(&b->d_pair2bra, b->h_pair2bra.data(), b->h_pair2bra.size()));
     CUDA_TRY(upload(&b->d_pair2ket, b->h_pair2ket.data(), b->h_pair2ket.size()));
     CUDA_TRY(upload(&b->d_log_q, b->h_log_q.data(), b->h_log_q.size()));
+    CUDA_TRY(upload(&b->d_log_q_raw, b->h_log_q_raw.data(), b->h_log_q_raw.size()));
     // class quartets (cp_ij >= cp_kl), each with its slice of the qoff buffer
     for (int cij = 0; cij < b->ncp; cij++)
         for (int ckl = 0; ckl <= cij; ckl++) {
@@ -563,6 +623,9 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
     CUDA_TRY(upload(&b->d_cq, b->h_cq.data(), b->h_cq.size()));
     CUDA_TRY(cudaMalloc(&b->d_qoff, sizeof(long long) * (b->qoff_total ? b->qoff_total : 1)));
     CUDA_TRY(cudaMalloc(&b->d_task0, sizeof(long long) * 2 * (b->ncq ? b->ncq : 1)));
+    CUDA_TRY(cudaMalloc(&b->d_qoff32, sizeof(long long) * (b->qoff_total ? b->qoff_total : 1)));
+    CUDA_TRY(cudaMalloc(&b->d_task032, sizeof(long long) * 2 * (b->ncq ? b->ncq : 1)));
+    CUDA_TRY(cudaMalloc(&b->d_klb, sizeof(int) * (b->qoff_total ? b->qoff_total : 1)));
     CUDA_TRY(cudaMalloc(&b->d_dm_cond, sizeof(double) * ngroups * ngroups));
     CUDA_TRY(cudaMalloc(&b->d_task01, sizeof(long long) * 2));
     return JK_OK;
@@ -618,6 +681,7 @@ static void fill_seg(const jk_basis* b, int cp_ij, int cp_kl, const long long* q
                      int n_dm, double* vj, double* vk, JKSeg* s) {
     s->rys = b->rys;
     s->qoff = qoff;
+    s->kl_base = nullptr;
     s->n_ij = n_ij;
     s->pair_ij0 = b->h_pair_locs[cp_ij];
     s->pair_kl0 = b->h_pair_locs[cp_kl];
@@ -661,8 +725,10 @@ extern "C" int jk_build(jk_basis_t* b, const double* dm, int n_dm, double* vj, d
     jk_dm_cond_kernel<<<gg, 256, 0, st>>>(dm, b->nao, n_dm, b->d_group_ao, b->ngroups, b->d_dm_cond);
     CUDA_TRY(cudaGetLastError());
     if (b->ncq == 0) return JK_OK;
-    jk_screen_kernel<<<b->ncq, 256, 0, st>>>(b->d_cq, b->d_log_q, b->d_dm_cond, b->ngroups, tol, nbins, prescreen,
-                                            b->d_qoff, b->d_task0);
+    double fp32_cutoff = opts ? opts->fp32_cutoff : 0.;
+    jk_screen_kernel<<<b->ncq, 256, 0, st>>>(b->d_cq, b->d_log_q, b->d_log_q_raw, b->d_dm_cond, b->ngroups, tol,
+                                            nbins, prescreen, fp32_cutoff, b->d_qoff, b->d_task0, b->d_qoff32,
+                                            b->d_task032, b->d_klb);
     CUDA_TRY(cudaGetLastError());
     for (int c = 0; c < b->ncq; c++) {
         const JKScreenCQ& cq = b->h_cq[c];
@@ -670,9 +736,17 @@ extern "C" int jk_build(jk_basis_t* b, const double* dm, int n_dm, double* vj, d
         fill_seg(b, cq.cp_ij, cq.cp_kl, b->d_qoff + cq.qoff_off, cq.n_ij, dm, n_dm, vj, vk, &seg);
         long long maxt = cq.cp_ij == cq.cp_kl ? (long long)cq.n_ij * (cq.n_ij + 1) / 2
                                               : (long long)cq.n_ij * cq.n_kl;
-        jk_launch_fn fn = g_tab64[class_index(b, cq.cp_ij, cq.cp_kl)];
+        int ci = class_index(b, cq.cp_ij, cq.cp_kl);
+        jk_launch_fn fn = g_tab64[ci];
         if (!fn) return set_err(JK_ERR_UNSUPPORTED, "no kernel for class quartet %d", c);
         CUDA_TRY(fn(seg, b->d_task0 + 2 * c, maxt, b->nsm, st));
+        if (fp32_cutoff > 0) {
+            jk_launch_fn f32 = g_tab32[ci];
+            if (!f32) return set_err(JK_ERR_UNSUPPORTED, "no FP32 kernel for class quartet %d", c);
+            seg.qoff = b->d_qoff32 + cq.qoff_off;
+            seg.kl_base = b->d_klb + cq.qoff_off;
+            CUDA_TRY(f32(seg, b->d_task032 + 2 * c, maxt, b->nsm, st));
+        }
     }
     return JK_OK;
 }
@@ -812,11 +886,17 @@ extern "C" int jk_basis_cq_info(const jk_basis_t* b, int* out) {
 extern "C" int jk_last_counts(const jk_basis_t* b, long long* out, void* stream) {
     if (!b || !out) return set_err(JK_ERR_ARG, "jk_last_counts: invalid arguments");
     if (b->ncq == 0) return JK_OK;
-    std::vector<long long> t(2 * (size_t)b->ncq);
+    std::vector<long long> t(2 * (size_t)b->ncq), t32(2 * (size_t)b->ncq);
     CUDA_TRY(cudaMemcpyAsync(t.data(), b->d_task0, sizeof(long long) * t.size(), cudaMemcpyDeviceToHost,
                              (cudaStream_t)stream));
+    CUDA_TRY(cudaMemcpyAsync(t32.data(), b->d_task032, sizeof(long long) * t32.size(), cudaMemcpyDeviceToHost,
+                             (cudaStream_t)stream));
     CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
-    for (int c = 0; c < b->ncq; c++) out[c] = t[2 * c + 1];
+    // FP64 quartets in out[0..ncq), FP32 quartets (mixed mode) in out[ncq..2 ncq)
+    for (int c = 0; c < b->ncq; c++) {
+        out[c] = t[2 * c + 1];
+        out[b->ncq + c] = t32[2 * c + 1];
+    }
     return JK_OK;
 }
 

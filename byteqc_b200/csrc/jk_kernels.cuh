@@ -50,6 +50,7 @@ struct JKQuartet {
 
 __device__ __forceinline__ JKQuartet jk_quartet_at(const JKSeg& sg, int row, int col) {
     JKQuartet q;
+    if (sg.kl_base) col += __ldg(sg.kl_base + row);
     int bij = sg.pair_ij0 + row, bkl = sg.pair_kl0 + col;
     q.ish = __ldg(sg.pair2bra + bij);
     q.jsh = __ldg(sg.pair2ket + bij);
@@ -419,7 +420,8 @@ __global__ void jk_team_kernel(const __grid_constant__ JKSeg sg0, const long lon
         JKQuartet q;
         double ri[3], rj[3], rk[3], rl[3];
         if (active) {
-            q = jk_quartet_at(sg, cur.row, cur.seek(sg, t));
+            const int col = cur.seek(sg, t);  // advances cur.row: evaluate first
+            q = jk_quartet_at(sg, cur.row, col);
             load_center(sg, q.ish, ri);
             load_center(sg, q.jsh, rj);
             load_center(sg, q.ksh, rk);

@@ -46,7 +46,7 @@ cudaError_t jk_launch(const JKSeg& seg, const long long* task0, long long max_ta
 // per-instantiation-file registration (jk_inst_*.cu, generated list)
 #include "jk_inst_list.h"
 
-#ifdef JK_WITH_FP32
+#ifndef JK_NO_FP32
 #define JK_REG32(LI, LJ, LK, LL) tab32[(LI)*64 + (LJ)*16 + (LK)*4 + (LL)] = jk_launch<LI, LJ, LK, LL, float>;
 #else
 #define JK_REG32(LI, LJ, LK, LL)

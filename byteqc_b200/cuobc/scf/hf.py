@@ -208,8 +208,13 @@ class _VHFOpt:
 
 def get_jk(mol, dm, hermi=1, vhfopt=None, with_j=True, with_k=True,
            omega=None, verbose=None, group_size=None, gpus=None,
-           prescreen=True, nbins=None, out='host'):
-    """Coulomb and exchange matrices of the density matrices ``dm``."""
+           prescreen=True, nbins=None, out='host', fp32_cutoff=None):
+    """Coulomb and exchange matrices of the density matrices ``dm``.
+
+    ``fp32_cutoff``: mixed precision -- contracted quartets whose screened
+    bound q_ij q_kl max|D| is below it run the Rys recursion and products in
+    FP32 (roots, weights, prefactors and all J/K accumulation stay FP64);
+    None or 0 keeps everything in FP64 (the reference's arithmetic)."""
     if hermi != 1:
         raise NotImplementedError(
             'JK-builder only supports hermitian density matrix')
@@ -233,6 +238,7 @@ def get_jk(mol, dm, hermi=1, vhfopt=None, with_j=True, with_k=True,
     opts.direct_scf_tol = vhfopt.direct_scf_tol
     opts.nbins = nbins if nbins is not None else vhfopt.default_nbins()
     opts.prescreen = int(bool(prescreen))
+    opts.fp32_cutoff = float(fp32_cutoff or 0.)
     _lib.check(lib.jk_get_jk(
         vhfopt.handle, vhfopt.coeff_dev.data_ptr(), nao0, d.data_ptr(), n_dm,
         vj.data_ptr() if with_j else None, vk.data_ptr() if with_k else None,

@@ -129,8 +129,10 @@ int jk_rys_roots_device(int n, const double *x, int count, double *s, double *w,
  * nprim_kl.  No reference counterpart: introspection for the cost model. */
 int jk_basis_cq_info(const jk_basis_t *basis, int *out);
 
-/* Screened contracted-quartet count per class quartet of the last jk_build
- * (synchronises `stream`).  No reference counterpart. */
+/* Screened contracted-quartet counts of the last jk_build (synchronises
+ * `stream`): out[c] the FP64 quartets of class quartet c, out[ncq + c] its
+ * FP32 quartets (mixed mode; 0 otherwise).  out has 2*ncq entries.  No
+ * reference counterpart. */
 int jk_last_counts(const jk_basis_t *basis, long long *out, void *stream);
 
 /* Measured FMA-pipe peak of the current device in TFLOP/s (fp32 = 0: FP64,

@@ -106,3 +106,21 @@ def test_device_rys_tables_match_host():
                 lib.jk_rys_roots_host(n, x, hs.ctypes.data, hw.ctypes.data)
                 np.testing.assert_allclose(s[i], hs, rtol=1e-14, atol=1e-300)
                 np.testing.assert_allclose(w[i], hw, rtol=1e-14, atol=1e-300)
+
+
+def test_mixed_precision_error_bounded():
+    """FP32 recursion below the cutoff: J/K stay within a bound that scales
+    with the cutoff, and fp32_cutoff=0 reproduces the FP64 engine exactly."""
+    from byteqc_b200.cuobc.scf import hf
+    from byteqc_b200.gto import geom as g
+    mol = _mol(4, 'standin-cc-pvdz', 7.0, seed=3)
+    s = mol.intor('int1e_ovlp')
+    dm = g.scf_like_density(s, nocc=mol.nelectron // 2, seed=1)
+    opt = hf._VHFOpt(mol).build()
+    vj, vk = hf.get_jk(mol, dm, vhfopt=opt)
+    vj0, vk0 = hf.get_jk(mol, dm, vhfopt=opt, fp32_cutoff=0.)
+    assert abs(vj0 - vj).max() < 1e-11 and abs(vk0 - vk).max() < 1e-11
+    for cut in (1e-8, 1e-6, 1e-4):
+        mj, mk = hf.get_jk(mol, dm, vhfopt=opt, fp32_cutoff=cut)
+        err = max(abs(mj - vj).max(), abs(mk - vk).max())
+        assert err < 100 * cut, (cut, err)
