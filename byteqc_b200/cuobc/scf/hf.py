@@ -265,3 +265,129 @@ def _get_jk(mf, mol=None, dm=None, hermi=1, with_j=True, with_k=True,
     if getattr(mf, '_opt_gpu', None) is None:
         mf._opt_gpu = _VHFOpt(mol, 'int2e').build(mf.direct_scf_tol)
     return get_jk(mol, dm, hermi, mf._opt_gpu, with_j, with_k)
+
+
+def eig(h, s):
+    """Generalised eigenproblem h C = s C e through Loewdin orthogonalisation
+    on the GPU (cuobc/scf/hf.py:253-265): functions with overlap eigenvalue
+    below 1e-15 are dropped."""
+    torch = _torch()
+    s = torch.as_tensor(s, dtype=torch.float64, device='cuda')
+    h = torch.as_tensor(h, dtype=torch.float64, device='cuda')
+    seig, t = torch.linalg.eigh(s)
+    keep = seig >= 1e-15
+    t = t[:, keep] / torch.sqrt(seig[keep])
+    e, c = torch.linalg.eigh(t.T @ h @ t)
+    return e, t @ c
+
+
+class RHF:
+    """Restricted Hartree-Fock driver around the J/K engine.
+
+    The reference's ``RHF`` (cuobc/scf/hf.py:272-274) overrides ``get_jk`` and
+    ``_eigh`` of PySCF's ``hf.RHF``; PySCF is not a dependency here, so this
+    class provides the loop itself: core-Hamiltonian guess, DIIS on the
+    orthogonalised commutator F D S - S D F, and direct-SCF incremental Fock
+    builds (J/K of the density change added to the previous ones, rebuilt from
+    scratch every ``rebuild_every`` cycles), all on the GPU.  ``fp32_cutoff``
+    switches on the mixed-precision engine.
+    """
+
+    def __init__(self, mol, fp32_cutoff=None):
+        self.mol = mol
+        self.conv_tol = 1e-9
+        self.conv_tol_grad = None
+        self.max_cycle = 60
+        self.direct_scf = True
+        self.direct_scf_tol = 1e-13
+        self.diis_space = 8
+        self.rebuild_every = 8
+        self.fp32_cutoff = fp32_cutoff
+        self.converged = False
+        self.e_tot = None
+        self.cycles = 0
+        self.jk_builds = 0
+        self._opt_gpu = None
+
+    def get_jk(self, mol=None, dm=None, hermi=1, with_j=True, with_k=True,
+               omega=None):
+        if omega is not None:
+            raise NotImplementedError('Range separated Coulomb integrals')
+        if mol is None:
+            mol = self.mol
+        if self._opt_gpu is None:
+            self._opt_gpu = _VHFOpt(mol, 'int2e').build(self.direct_scf_tol)
+        self.jk_builds += 1
+        return get_jk(mol, dm, hermi, self._opt_gpu, with_j, with_k,
+                      out='device', fp32_cutoff=self.fp32_cutoff)
+
+    def eig(self, h, s):
+        return eig(h, s)
+
+    def kernel(self, dm0=None):
+        torch = _torch()
+        mol = self.mol
+        dev = dict(dtype=torch.float64, device='cuda')
+        s = torch.as_tensor(mol.intor('int1e_ovlp'), **dev)
+        h = torch.as_tensor(mol.intor('int1e_kin') + mol.intor('int1e_nuc'),
+                            **dev)
+        e_nuc = mol.energy_nuc()
+        nocc = mol.nelectron // 2
+        if dm0 is None:
+            _, c = self.eig(h, s)
+            dm = 2. * c[:, :nocc] @ c[:, :nocc].T
+        else:
+            dm = torch.as_tensor(dm0, **dev)
+        seig, t = torch.linalg.eigh(s)
+        x = t[:, seig >= 1e-15] / torch.sqrt(seig[seig >= 1e-15])
+        vj = vk = None
+        dm_last = None
+        fs, es = [], []
+        e_last = None
+        self.converged = False
+        for cycle in range(1, self.max_cycle + 1):
+            if (self.direct_scf and dm_last is not None
+                    and cycle % self.rebuild_every != 0):
+                dj, dk = self.get_jk(mol, dm - dm_last)
+                vj, vk = vj + dj, vk + dk
+            else:
+                vj, vk = self.get_jk(mol, dm)
+            f = h + vj - .5 * vk
+            e_tot = float(.5 * torch.sum(dm * (h + f))) + e_nuc
+            err = x.T @ (f @ dm @ s - s @ dm @ f) @ x
+            fs.append(f)
+            es.append(err)
+            if len(fs) > self.diis_space:
+                fs.pop(0)
+                es.pop(0)
+            n = len(fs)
+            if n > 1:
+                b = torch.empty(n + 1, n + 1, **dev)
+                b[-1, :] = -1
+                b[:, -1] = -1
+                b[-1, -1] = 0
+                for i in range(n):
+                    for j in range(i + 1):
+                        b[i, j] = b[j, i] = torch.sum(es[i] * es[j])
+                rhs = torch.zeros(n + 1, **dev)
+                rhs[-1] = -1
+                coef = torch.linalg.lstsq(b, rhs[:, None]).solution[:n, 0]
+                f = sum(ci * fi for ci, fi in zip(coef, fs))
+            mo_e, c = self.eig(f, s)
+            dm_last = dm
+            dm = 2. * c[:, :nocc] @ c[:, :nocc].T
+            grad = float(err.abs().max())
+            self.cycles = cycle
+            if e_last is not None and abs(e_tot - e_last) < self.conv_tol and (
+                    self.conv_tol_grad is None or grad < self.conv_tol_grad):
+                self.converged = True
+                self.e_tot = e_tot
+                break
+            e_last = e_tot
+        # final energy of the converged density with a full (non-incremental) build
+        vj, vk = self.get_jk(mol, dm)
+        f = h + vj - .5 * vk
+        self.e_tot = float(.5 * torch.sum(dm * (h + f))) + e_nuc
+        self.mo_energy, self.mo_coeff = mo_e.cpu().numpy(), c.cpu().numpy()
+        self.make_rdm1 = lambda: dm.cpu().numpy()
+        return self.e_tot
