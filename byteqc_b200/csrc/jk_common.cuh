@@ -338,3 +338,9 @@ struct JKSeg {
     double* vj;
     double* vk;
 };
+
+// launchers of one class: a single segment (by value) or a segment table
+typedef cudaError_t (*jk_launch_fn)(const JKSeg& seg, const long long* task0, long long max_tasks, int nsm,
+                                    cudaStream_t st);
+typedef cudaError_t (*jk_launch_batch_fn)(const JKSeg* segs, const long long* segt, int nseg, long long max_tasks,
+                                          int nsm, cudaStream_t st);

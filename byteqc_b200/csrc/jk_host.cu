@@ -43,7 +43,9 @@ extern "C" const char* jk_last_error(void) { return g_err.c_str(); }
 // ---------------------------------------------------------------------------
 // launcher tables
 // ---------------------------------------------------------------------------
-static jk_launch_fn g_tab64[256], g_tab32[256];
+static JKTables g_tabs;
+#define g_tab64 g_tabs.t64
+#define g_tab32 g_tabs.t32
 static std::once_flag g_tab_once;
 static void init_tables() {
     std::call_once(g_tab_once, [] {
@@ -186,12 +188,6 @@ __global__ void jk_dm_cond_kernel(const double* __restrict__ dm, int nao, int n_
     if (threadIdx.x == 0) out[gi * ngroups + gj] = red[0];
 }
 
-struct JKScreenCQ {
-    int cp_ij, cp_kl;
-    int gi, gj, gk, gl;
-    int pair_ij0, n_ij, pair_kl0, n_kl;
-    long long qoff_off;
-};
 
 // Block-wide inclusive scan of two counts (256 threads), with running carries.
 __device__ __forceinline__ void jk_block_scan2(long long a, long long b, long long& ia, long long& ib,
@@ -247,17 +243,14 @@ __device__ __forceinline__ void jk_block_scan2(long long a, long long b, long lo
 // at the bound q_ij q_kl sub = fp32_cutoff (unclipped log q); the leading
 // part (larger bounds) runs in FP64, the tail in FP32.  qoff counts the FP64
 // part, qoff32 the FP32 part, whose first column per row is klb[ij].
-__global__ void jk_screen_kernel(const JKScreenCQ* __restrict__ cqs, const double* __restrict__ log_q,
-                                 const double* __restrict__ log_q_raw, const double* __restrict__ dm_cond,
-                                 int ngroups, double tol, int nbins, int prescreen, double fp32_cutoff,
-                                 long long* __restrict__ qoff_all, long long* __restrict__ task0_all,
-                                 long long* __restrict__ qoff32_all, long long* __restrict__ task032_all,
-                                 int* __restrict__ klb_all) {
+__global__ void jk_screen_kernel(const JKScreenCQ* __restrict__ cqs, double tol, int nbins, int prescreen,
+                                 double fp32_cutoff) {
     const JKScreenCQ cq = cqs[blockIdx.x];
-    long long* qoff = qoff_all + cq.qoff_off;
-    long long* qoff32 = qoff32_all + cq.qoff_off;
-    int* klb = klb_all + cq.qoff_off;
-    const double* c = dm_cond;
+    long long* qoff = cq.qoff;
+    long long* qoff32 = cq.qoff32;
+    int* klb = cq.klb;
+    const double* c = cq.dm_cond;
+    const int ngroups = cq.ngroups;
     double sub = fmax(fmax(fmax(c[cq.gi * ngroups + cq.gj], c[cq.gk * ngroups + cq.gl]),
                            fmax(c[cq.gi * ngroups + cq.gk], c[cq.gj * ngroups + cq.gk])),
                       fmax(c[cq.gi * ngroups + cq.gl], c[cq.gj * ngroups + cq.gl]));
@@ -266,10 +259,10 @@ __global__ void jk_screen_kernel(const JKScreenCQ* __restrict__ cqs, const doubl
     double scale = nbins / log(fmin(cutoff, 0.1));
     const bool mixed = fp32_cutoff > 0;
     const double log_thr = mixed ? log(fp32_cutoff / sub) : 0.;  // q_ij q_kl >= fp32_cutoff / sub
-    const double* lq_ij = log_q + cq.pair_ij0;
-    const double* lq_kl = log_q + cq.pair_kl0;
-    const double* rq_ij = log_q_raw + cq.pair_ij0;
-    const double* rq_kl = log_q_raw + cq.pair_kl0;
+    const double* lq_ij = cq.lq_ij;
+    const double* lq_kl = cq.lq_kl;
+    const double* rq_ij = cq.rq_ij;
+    const double* rq_kl = cq.rq_kl;
     bool diag = cq.cp_ij == cq.cp_kl;
     __shared__ long long carry, carry32;
     __shared__ long long wsum[32], wsum32[32];
@@ -316,10 +309,10 @@ __global__ void jk_screen_kernel(const JKScreenCQ* __restrict__ cqs, const doubl
         }
     }
     if (threadIdx.x == 0) {
-        task0_all[2 * blockIdx.x] = 0;
-        task0_all[2 * blockIdx.x + 1] = carry;
-        task032_all[2 * blockIdx.x] = 0;
-        task032_all[2 * blockIdx.x + 1] = carry32;
+        cq.task0[0] = 0;
+        cq.task0[1] = carry;
+        cq.task032[0] = 0;
+        cq.task032[1] = carry32;
     }
 }
 
@@ -340,39 +333,6 @@ __global__ void jk_symmetrize_kernel(const double* __restrict__ in, double* __re
 // ---------------------------------------------------------------------------
 // basis object
 // ---------------------------------------------------------------------------
-struct jk_basis {
-    int device = 0, nsm = 148;
-    const double* rys = nullptr;  // shared per-device Rys table
-    int natm = 0, nbas = 0, nao = 0, ngroups = 0, ncp = 0, ncq = 0;
-    double diag_fac = 0.5, cutoff = 1e-13;
-    std::vector<int> h_ao_loc, h_group_off, h_group_l, h_group_nprim;
-    std::vector<int> h_cls_gi, h_cls_gj, h_pair_locs, h_prim_locs, h_pair2bra, h_pair2ket;
-    std::vector<double> h_log_q, h_log_q_raw, h_qcond;
-    std::vector<JKScreenCQ> h_cq;
-    std::vector<long long> h_qoff_off;
-    long long qoff_total = 0;
-    // device
-    int *d_atm = nullptr, *d_bas = nullptr, *d_ao_loc = nullptr, *d_group_ao = nullptr;
-    double *d_env = nullptr, *d_bas_x = nullptr, *d_qcond = nullptr;
-    int *d_pair2bra = nullptr, *d_pair2ket = nullptr;
-    double *d_log_q = nullptr, *d_log_q_raw = nullptr, *d_prim = nullptr;  // prim: a12|e12|x12|y12|z12
-    long long nprim_total = 0;
-    JKScreenCQ* d_cq = nullptr;
-    long long *d_qoff = nullptr, *d_task0 = nullptr;
-    long long *d_qoff32 = nullptr, *d_task032 = nullptr;  // FP32 part of the mixed mode
-    int* d_klb = nullptr;
-    double* d_dm_cond = nullptr;
-    // reference-compatible single class-pair path
-    long long* d_qoff1 = nullptr;
-    long long* d_task01 = nullptr;
-    long long qoff1_cap = 0;
-    long long* h_qoff1 = nullptr;  // pinned
-    size_t h_qoff1_cap = 0;
-    // transform workspace
-    cublasHandle_t blas = nullptr;
-    double* d_work = nullptr;
-    size_t work_cap = 0;
-};
 
 static void free_basis(jk_basis* b) {
     if (!b) return;
@@ -620,13 +580,27 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
             b->h_cq.push_back(c);
         }
     b->ncq = (int)b->h_cq.size();
-    CUDA_TRY(upload(&b->d_cq, b->h_cq.data(), b->h_cq.size()));
     CUDA_TRY(cudaMalloc(&b->d_qoff, sizeof(long long) * (b->qoff_total ? b->qoff_total : 1)));
     CUDA_TRY(cudaMalloc(&b->d_task0, sizeof(long long) * 2 * (b->ncq ? b->ncq : 1)));
     CUDA_TRY(cudaMalloc(&b->d_qoff32, sizeof(long long) * (b->qoff_total ? b->qoff_total : 1)));
     CUDA_TRY(cudaMalloc(&b->d_task032, sizeof(long long) * 2 * (b->ncq ? b->ncq : 1)));
     CUDA_TRY(cudaMalloc(&b->d_klb, sizeof(int) * (b->qoff_total ? b->qoff_total : 1)));
     CUDA_TRY(cudaMalloc(&b->d_dm_cond, sizeof(double) * ngroups * ngroups));
+    for (int c = 0; c < b->ncq; c++) {
+        JKScreenCQ& q = b->h_cq[c];
+        q.ngroups = ngroups;
+        q.lq_ij = b->d_log_q + q.pair_ij0;
+        q.lq_kl = b->d_log_q + q.pair_kl0;
+        q.rq_ij = b->d_log_q_raw + q.pair_ij0;
+        q.rq_kl = b->d_log_q_raw + q.pair_kl0;
+        q.dm_cond = b->d_dm_cond;
+        q.qoff = b->d_qoff + q.qoff_off;
+        q.qoff32 = b->d_qoff32 + q.qoff_off;
+        q.klb = b->d_klb + q.qoff_off;
+        q.task0 = b->d_task0 + 2 * c;
+        q.task032 = b->d_task032 + 2 * c;
+    }
+    CUDA_TRY(upload(&b->d_cq, b->h_cq.data(), b->h_cq.size()));
     CUDA_TRY(cudaMalloc(&b->d_task01, sizeof(long long) * 2));
     return JK_OK;
 }
@@ -707,6 +681,7 @@ static void fill_seg(const jk_basis* b, int cp_ij, int cp_kl, const long long* q
     s->vk = vk;
 }
 
+int jk_internal_class_index(const jk_basis_t* b, int cp_ij, int cp_kl);
 static int class_index(const jk_basis* b, int cp_ij, int cp_kl) {
     int li = b->h_group_l[b->h_cls_gi[cp_ij]], lj = b->h_group_l[b->h_cls_gj[cp_ij]];
     int lk = b->h_group_l[b->h_cls_gi[cp_kl]], ll = b->h_group_l[b->h_cls_gj[cp_kl]];
@@ -726,9 +701,7 @@ extern "C" int jk_build(jk_basis_t* b, const double* dm, int n_dm, double* vj, d
     CUDA_TRY(cudaGetLastError());
     if (b->ncq == 0) return JK_OK;
     double fp32_cutoff = opts ? opts->fp32_cutoff : 0.;
-    jk_screen_kernel<<<b->ncq, 256, 0, st>>>(b->d_cq, b->d_log_q, b->d_log_q_raw, b->d_dm_cond, b->ngroups, tol,
-                                            nbins, prescreen, fp32_cutoff, b->d_qoff, b->d_task0, b->d_qoff32,
-                                            b->d_task032, b->d_klb);
+    jk_screen_kernel<<<b->ncq, 256, 0, st>>>(b->d_cq, tol, nbins, prescreen, fp32_cutoff);
     CUDA_TRY(cudaGetLastError());
     for (int c = 0; c < b->ncq; c++) {
         const JKScreenCQ& cq = b->h_cq[c];
@@ -1036,5 +1009,27 @@ int jk_internal_launch(const jk_basis_t* b, int cp_ij, int cp_kl, const JKSeg& s
     jk_launch_fn fn = g_tab64[class_index(b, cp_ij, cp_kl)];
     if (!fn) return set_err(JK_ERR_UNSUPPORTED, "no kernel for class pair (%d, %d)", cp_ij, cp_kl);
     CUDA_TRY(fn(seg, d_task0, max_tasks, b->nsm, (cudaStream_t)stream));
+    return JK_OK;
+}
+
+int jk_internal_class_index(const jk_basis_t* b, int cp_ij, int cp_kl) { return class_index(b, cp_ij, cp_kl); }
+
+jk_launch_batch_fn jk_internal_batch_launcher(int class_idx, int fp32) {
+    init_tables();
+    return fp32 ? g_tabs.b32[class_idx] : g_tabs.b64[class_idx];
+}
+
+void jk_internal_fill_seg_batch(const jk_basis_t* b, int c, const double* dm, int n_dm, double* vj, double* vk,
+                                int fp32, JKSeg* out) {
+    const JKScreenCQ& cq = b->h_cq[c];
+    fill_seg(b, cq.cp_ij, cq.cp_kl, fp32 ? cq.qoff32 : cq.qoff, cq.n_ij, dm, n_dm, vj, vk, out);
+    if (fp32) out->kl_base = cq.klb;
+}
+
+int jk_internal_screen(const JKScreenCQ* d_cq, int ncq, double tol, int nbins, int prescreen, double fp32_cutoff,
+                       void* stream) {
+    if (ncq <= 0) return JK_OK;
+    jk_screen_kernel<<<ncq, 256, 0, (cudaStream_t)stream>>>(d_cq, tol, nbins, prescreen, fp32_cutoff);
+    CUDA_TRY(cudaGetLastError());
     return JK_OK;
 }

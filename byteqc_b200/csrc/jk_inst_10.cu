@@ -2,9 +2,8 @@
 // file per slice so the build compiles them in parallel).
 #include "jk_launch.cuh"
 
-void jk_register_10(jk_launch_fn* tab64, jk_launch_fn* tab32) {
+void jk_register_10(JKTables* T) {
     JK_REG(1, 0, 0, 0)
     JK_REG(1, 0, 1, 0)
     JK_REG(1, 0, 1, 1)
-    (void)tab32;
 }

@@ -2,12 +2,11 @@
 // file per slice so the build compiles them in parallel).
 #include "jk_launch.cuh"
 
-void jk_register_21(jk_launch_fn* tab64, jk_launch_fn* tab32) {
+void jk_register_21(JKTables* T) {
     JK_REG(2, 1, 0, 0)
     JK_REG(2, 1, 1, 0)
     JK_REG(2, 1, 1, 1)
     JK_REG(2, 1, 2, 0)
     JK_REG(2, 1, 2, 1)
     JK_REG(2, 1, 2, 2)
-    (void)tab32;
 }

@@ -2,9 +2,8 @@
 // file per slice so the build compiles them in parallel).
 #include "jk_launch.cuh"
 
-void jk_register_302(jk_launch_fn* tab64, jk_launch_fn* tab32) {
+void jk_register_302(JKTables* T) {
     JK_REG(3, 0, 2, 0)
     JK_REG(3, 0, 2, 1)
     JK_REG(3, 0, 2, 2)
-    (void)tab32;
 }

@@ -2,8 +2,7 @@
 // file per slice so the build compiles them in parallel).
 #include "jk_launch.cuh"
 
-void jk_register_311(jk_launch_fn* tab64, jk_launch_fn* tab32) {
+void jk_register_311(JKTables* T) {
     JK_REG(3, 1, 1, 0)
     JK_REG(3, 1, 1, 1)
-    (void)tab32;
 }

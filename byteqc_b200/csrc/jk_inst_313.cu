@@ -2,10 +2,9 @@
 // file per slice so the build compiles them in parallel).
 #include "jk_launch.cuh"
 
-void jk_register_313(jk_launch_fn* tab64, jk_launch_fn* tab32) {
+void jk_register_313(JKTables* T) {
     JK_REG(3, 1, 3, 0)
     JK_REG(3, 1, 3, 1)
     JK_REG(3, 1, 3, 2)
     JK_REG(3, 1, 3, 3)
-    (void)tab32;
 }

@@ -2,7 +2,6 @@
 // file per slice so the build compiles them in parallel).
 #include "jk_launch.cuh"
 
-void jk_register_320(jk_launch_fn* tab64, jk_launch_fn* tab32) {
+void jk_register_320(JKTables* T) {
     JK_REG(3, 2, 0, 0)
-    (void)tab32;
 }

@@ -2,7 +2,6 @@
 // file per slice so the build compiles them in parallel).
 #include "jk_launch.cuh"
 
-void jk_register_330(jk_launch_fn* tab64, jk_launch_fn* tab32) {
+void jk_register_330(JKTables* T) {
     JK_REG(3, 3, 0, 0)
-    (void)tab32;
 }

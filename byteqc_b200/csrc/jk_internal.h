@@ -1,8 +1,32 @@
 // Internal helpers of jk_host.cu shared with other translation units of
 // libjk.so (not part of the C-ABI).
 #pragma once
+#include <cublas_v2.h>
+
+#include <string>
+#include <vector>
+
 #include "jk_common.cuh"
 #include "../../include/byteqc_jk.h"
+
+// One class quartet (cp_ij >= cp_kl) of one basis, as the screening kernel
+// sees it: pair counts, group indices and the device buffers it reads/writes.
+struct JKScreenCQ {
+    int cp_ij, cp_kl;
+    int gi, gj, gk, gl;
+    int n_ij, n_kl;
+    int ngroups;
+    const double *lq_ij, *lq_kl;  // clipped log q of the two classes
+    const double *rq_ij, *rq_kl;  // unclipped log q (mixed-precision split)
+    const double* dm_cond;        // ngroups x ngroups
+    long long *qoff, *qoff32;     // row prefixes, FP64 and FP32 parts
+    int* klb;                     // first FP32 column per row
+    long long *task0, *task032;   // {0, count} of each part
+    // host bookkeeping
+    int pair_ij0, pair_kl0;
+    long long qoff_off;
+};
+
 
 int jk_internal_set_err(int code, const char* msg);
 // pair counts of the two classes and the working-basis size
@@ -12,3 +36,47 @@ void jk_internal_fill_seg(const jk_basis_t* b, int cp_ij, int cp_kl, const long 
 // launch the class kernel of (cp_ij, cp_kl) on a device segment table of one entry
 int jk_internal_launch(const jk_basis_t* b, int cp_ij, int cp_kl, const JKSeg& seg, const long long* d_task0,
                        long long max_tasks, void* stream);
+
+// Per-geometry state (opaque to callers of the C-ABI)
+struct jk_basis {
+    // class quartets and their screening records
+    int device = 0, nsm = 148;
+    const double* rys = nullptr;  // shared per-device Rys table
+    int natm = 0, nbas = 0, nao = 0, ngroups = 0, ncp = 0, ncq = 0;
+    double diag_fac = 0.5, cutoff = 1e-13;
+    std::vector<int> h_ao_loc, h_group_off, h_group_l, h_group_nprim;
+    std::vector<int> h_cls_gi, h_cls_gj, h_pair_locs, h_prim_locs, h_pair2bra, h_pair2ket;
+    std::vector<double> h_log_q, h_log_q_raw, h_qcond;
+    std::vector<JKScreenCQ> h_cq;
+    std::vector<long long> h_qoff_off;
+    long long qoff_total = 0;
+    // device
+    int *d_atm = nullptr, *d_bas = nullptr, *d_ao_loc = nullptr, *d_group_ao = nullptr;
+    double *d_env = nullptr, *d_bas_x = nullptr, *d_qcond = nullptr;
+    int *d_pair2bra = nullptr, *d_pair2ket = nullptr;
+    double *d_log_q = nullptr, *d_log_q_raw = nullptr, *d_prim = nullptr;  // prim: a12|e12|x12|y12|z12
+    long long nprim_total = 0;
+    JKScreenCQ* d_cq = nullptr;
+    long long *d_qoff = nullptr, *d_task0 = nullptr;
+    long long *d_qoff32 = nullptr, *d_task032 = nullptr;  // FP32 part of the mixed mode
+    int* d_klb = nullptr;
+    double* d_dm_cond = nullptr;
+    // reference-compatible single class-pair path
+    long long* d_qoff1 = nullptr;
+    long long* d_task01 = nullptr;
+    long long qoff1_cap = 0;
+    long long* h_qoff1 = nullptr;  // pinned
+    size_t h_qoff1_cap = 0;
+    // transform workspace
+    cublasHandle_t blas = nullptr;
+    double* d_work = nullptr;
+    size_t work_cap = 0;
+};
+
+// launch one class quartet of basis b as a single segment
+int jk_internal_class_index(const jk_basis_t* b, int cp_ij, int cp_kl);
+jk_launch_batch_fn jk_internal_batch_launcher(int class_idx, int fp32);
+void jk_internal_fill_seg_batch(const jk_basis_t* b, int c, const double* dm, int n_dm, double* vj, double* vk,
+                                int fp32, JKSeg* out);
+int jk_internal_screen(const JKScreenCQ* d_cq, int ncq, double tol, int nbins, int prescreen, double fp32_cutoff,
+                       void* stream);

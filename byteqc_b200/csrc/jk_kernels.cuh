@@ -85,6 +85,58 @@ struct JKTaskCursor {
     }
 };
 
+// Task sources of a launch.  JKOneSeg: one segment passed by value in the
+// kernel's parameter space, task count at task0[1].  JKSegTable: several
+// segments (one per molecule of a batch) in global memory with exclusive task
+// prefix segt[0..nseg]; all segments of a launch share the class and the
+// primitive counts.  Cursors walk increasing task indices.
+struct JKOneSeg {
+    const JKSeg& sg;
+    const long long* task0;
+    __device__ __forceinline__ long long total() const { return task0[1]; }
+    __device__ __forceinline__ const JKSeg& first() const { return sg; }
+    struct Cursor {
+        JKTaskCursor rc;
+        __device__ __forceinline__ void init(const JKOneSeg& src, long long t) { rc.init(src.sg, t); }
+        // (segment, row, col) of task t
+        __device__ __forceinline__ const JKSeg& seek(const JKOneSeg& src, long long t, int& row, int& col) {
+            col = rc.seek(src.sg, t);
+            row = rc.row;
+            return src.sg;
+        }
+    };
+};
+
+struct JKSegTable {
+    const JKSeg* segs;
+    const long long* segt;
+    int nseg;
+    __device__ __forceinline__ long long total() const { return segt[nseg]; }
+    __device__ __forceinline__ const JKSeg& first() const { return segs[0]; }
+    struct Cursor {
+        int s;
+        long long sbeg, send;
+        JKTaskCursor rc;
+        __device__ __forceinline__ void init(const JKSegTable& src, long long t) {
+            s = jk_find_seg(src.segt, src.nseg, t);
+            sbeg = src.segt[s];
+            send = src.segt[s + 1];
+            rc.init(src.segs[s], t - sbeg);
+        }
+        __device__ __forceinline__ const JKSeg& seek(const JKSegTable& src, long long t, int& row, int& col) {
+            if (t >= send) {
+                while (t >= src.segt[s + 1]) s++;
+                sbeg = src.segt[s];
+                send = src.segt[s + 1];
+                rc.init(src.segs[s], t - sbeg);
+            }
+            col = rc.seek(src.segs[s], t - sbeg);
+            row = rc.row;
+            return src.segs[s];
+        }
+    };
+};
+
 // prefactors of one primitive quartet
 struct JKPrim {
     double x, A, B, AB, sy;  // Boys argument, exponent sums, y seed
@@ -302,15 +354,13 @@ __device__ __forceinline__ void jk_thread_quartet(const JKSeg& sg, const JKQuart
     jk_thread_passes<C, R, 0>(sg, q, tab, ri, rj, rk, rl);
 }
 
-template <class C, typename R>
-__global__ void __launch_bounds__(128, C::MINB) jk_thread_kernel(const __grid_constant__ JKSeg sg,
-                                                                 const long long* __restrict__ task0) {
-    extern __shared__ __align__(16) double jk_tab[];
-    rys_table_to_smem<C::NROOTS>(sg.rys, jk_tab);
+template <class C, typename R, class Src>
+__device__ __forceinline__ void jk_thread_body(const Src& src, double* jk_tab) {
+    rys_table_to_smem<C::NROOTS>(src.first().rys, jk_tab);
     __syncthreads();
     // each warp takes a contiguous chunk of tasks (a multiple of 32); lane i
     // does tasks i, i+32, ... of it, so a warp covers consecutive kl of a row
-    const long long total = task0[1];
+    const long long total = src.total();
     const int lane = threadIdx.x & 31;
     const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
     const long long wid = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -318,13 +368,31 @@ __global__ void __launch_bounds__(128, C::MINB) jk_thread_kernel(const __grid_co
     long long t = wid * chunk + lane;
     const long long tend = min(total, (wid + 1) * chunk);
     if (t >= tend) return;
-    JKTaskCursor cur;
-    cur.init(sg, t);
+    typename Src::Cursor cur;
+    cur.init(src, t);
     for (; t < tend; t += 32) {
-        int col = cur.seek(sg, t);
-        JKQuartet q = jk_quartet_at(sg, cur.row, col);
+        int row, col;
+        const JKSeg& sg = cur.seek(src, t, row, col);
+        JKQuartet q = jk_quartet_at(sg, row, col);
         jk_thread_quartet<C, R>(sg, q, jk_tab);
     }
+}
+
+template <class C, typename R>
+__global__ void __launch_bounds__(128, C::MINB) jk_thread_kernel(const __grid_constant__ JKSeg sg,
+                                                                 const long long* __restrict__ task0) {
+    extern __shared__ __align__(16) double jk_tab[];
+    JKOneSeg src{sg, task0};
+    jk_thread_body<C, R>(src, jk_tab);
+}
+
+template <class C, typename R>
+__global__ void __launch_bounds__(128, C::MINB) jk_thread_kernel_batch(const JKSeg* __restrict__ segs,
+                                                                       const long long* __restrict__ segt,
+                                                                       int nseg) {
+    extern __shared__ __align__(16) double jk_tab[];
+    JKSegTable src{segs, segt, nseg};
+    jk_thread_body<C, R>(src, jk_tab);
 }
 
 // ===========================================================================
@@ -375,8 +443,8 @@ __host__ __device__ constexpr size_t jk_team_smem() {
     return (size_t)S::TAB * sizeof(double) + jk_team_gbytes<C, R>() + (size_t)S::QPB * S::BWORDS * sizeof(double);
 }
 
-template <class C, typename R>
-__global__ void jk_team_kernel(const __grid_constant__ JKSeg sg0, const long long* __restrict__ task0) {
+template <class C, typename R, class Src>
+__device__ __forceinline__ void jk_team_body(const Src& src) {
     using S = JKTeamShape<C>;
     constexpr int T = C::T, NR = C::NROOTS;
     extern __shared__ __align__(16) unsigned char jk_smem[];
@@ -386,6 +454,7 @@ __global__ void jk_team_kernel(const __grid_constant__ JKSeg sg0, const long lon
     R* g = reinterpret_cast<R*>(gbase + (size_t)team * jk_team_region<C, R>());
     double* part = reinterpret_cast<double*>(g);  // digestion partials reuse the 2D-block space
     double* buf = reinterpret_cast<double*>(gbase + jk_team_gbytes<C, R>()) + (size_t)team * S::BWORDS;
+    const JKSeg& sg0 = src.first();
     if (S::SMEM_TAB) rys_table_to_smem<NR>(sg0.rys, tab);
 
     // owned Cartesian indices
@@ -403,25 +472,29 @@ __global__ void jk_team_kernel(const __grid_constant__ JKSeg sg0, const long lon
     }
 
     __syncthreads();
-    const JKSeg& sg = sg0;
-    const long long total = task0[1];
-    const int nprim_ij = sg.nprim_ij, nprim_kl = sg.nprim_kl;
+    const long long total = src.total();
+    const int nprim_ij = sg0.nprim_ij, nprim_kl = sg0.nprim_kl;  // uniform within a launch
     // each team takes a contiguous chunk of tasks; every team of the block
     // runs the same number of iterations (the block synchronises inside)
     const long long nteams = (long long)gridDim.x * S::QPB;
     const long long tid = (long long)blockIdx.x * S::QPB + team;
     const long long chunk = (total + nteams - 1) / nteams;
     const long long tbeg = tid * chunk, tend = min(total, tbeg + chunk);
-    JKTaskCursor cur;
-    if (tbeg < tend) cur.init(sg, tbeg);
+    typename Src::Cursor cur;
+    if (tbeg < tend) cur.init(src, tbeg);
     for (long long it = 0; it < chunk; it++) {
         const long long t = tbeg + it;
         const bool active = t < tend;
         JKQuartet q;
         double ri[3], rj[3], rk[3], rl[3];
+        const JKSeg* sgp = &sg0;
         if (active) {
-            const int col = cur.seek(sg, t);  // advances cur.row: evaluate first
-            q = jk_quartet_at(sg, cur.row, col);
+            int row, col;
+            sgp = &cur.seek(src, t, row, col);
+            q = jk_quartet_at(*sgp, row, col);
+        }
+        const JKSeg& sg = *sgp;
+        if (active) {
             load_center(sg, q.ish, ri);
             load_center(sg, q.jsh, rj);
             load_center(sg, q.ksh, rk);
@@ -681,5 +754,16 @@ __global__ void jk_team_kernel(const __grid_constant__ JKSeg sg0, const long lon
             __syncthreads();
         }
     }
+}
+template <class C, typename R>
+__global__ void jk_team_kernel(const __grid_constant__ JKSeg sg, const long long* __restrict__ task0) {
+    JKOneSeg src{sg, task0};
+    jk_team_body<C, R>(src);
+}
+
+template <class C, typename R>
+__global__ void jk_team_kernel_batch(const JKSeg* __restrict__ segs, const long long* __restrict__ segt, int nseg) {
+    JKSegTable src{segs, segt, nseg};
+    jk_team_body<C, R>(src);
 }
 #undef DM

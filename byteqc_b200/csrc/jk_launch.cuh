@@ -3,8 +3,6 @@
 #pragma once
 #include "jk_kernels.cuh"
 
-typedef cudaError_t (*jk_launch_fn)(const JKSeg& seg, const long long* task0, long long max_tasks, int nsm,
-                                    cudaStream_t st);
 
 // One class quartet (one segment): the segment descriptor goes by value into
 // the kernel's parameter space; task0[1] (device) holds the task count.
@@ -43,14 +41,62 @@ cudaError_t jk_launch(const JKSeg& seg, const long long* task0, long long max_ta
     return cudaGetLastError();
 }
 
+// Batched launch: the segments of one class (same angular momenta and
+// primitive counts) of many molecules, task prefix segt[0..nseg] on the device.
+
+template <int LI, int LJ, int LK, int LL, typename R>
+cudaError_t jk_launch_batch(const JKSeg* segs, const long long* segt, int nseg, long long max_tasks, int nsm,
+                            cudaStream_t st) {
+    using C = JKClass<LI, LJ, LK, LL>;
+    if (max_tasks <= 0 || nseg <= 0) return cudaSuccess;
+    if constexpr (C::P == 0) {
+        constexpr size_t smem = RysS<C::NROOTS>::WORDS * sizeof(double);
+        static bool attr_set = false;
+        if (!attr_set) {
+            cudaError_t e = cudaFuncSetAttribute(jk_thread_kernel_batch<C, R>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            attr_set = true;
+        }
+        long long want = (max_tasks + 127) / 128;
+        long long cap = (long long)nsm * 16;
+        int blocks = (int)(want < cap ? want : cap);
+        jk_thread_kernel_batch<C, R><<<blocks, 128, smem, st>>>(segs, segt, nseg);
+    } else {
+        using S = JKTeamShape<C>;
+        constexpr size_t smem = jk_team_smem<C, R>();
+        static bool attr_set = false;
+        if (!attr_set) {
+            cudaError_t e = cudaFuncSetAttribute(jk_team_kernel_batch<C, R>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            attr_set = true;
+        }
+        long long want = (max_tasks + S::QPB - 1) / S::QPB;
+        long long cap = (long long)nsm * 8;
+        int blocks = (int)(want < cap ? want : cap);
+        jk_team_kernel_batch<C, R><<<blocks, S::THREADS, smem, st>>>(segs, segt, nseg);
+    }
+    return cudaGetLastError();
+}
+
+// launcher tables indexed by li*64 + lj*16 + lk*4 + ll
+struct JKTables {
+    jk_launch_fn t64[256], t32[256];
+    jk_launch_batch_fn b64[256], b32[256];
+};
+
 // per-instantiation-file registration (jk_inst_*.cu, generated list)
 #include "jk_inst_list.h"
 
 #ifndef JK_NO_FP32
-#define JK_REG32(LI, LJ, LK, LL) tab32[(LI)*64 + (LJ)*16 + (LK)*4 + (LL)] = jk_launch<LI, LJ, LK, LL, float>;
+#define JK_REG32(LI, LJ, LK, LL)                                         \
+    T->t32[(LI)*64 + (LJ)*16 + (LK)*4 + (LL)] = jk_launch<LI, LJ, LK, LL, float>; \
+    T->b32[(LI)*64 + (LJ)*16 + (LK)*4 + (LL)] = jk_launch_batch<LI, LJ, LK, LL, float>;
 #else
 #define JK_REG32(LI, LJ, LK, LL)
 #endif
-#define JK_REG(LI, LJ, LK, LL)                                                     \
-    tab64[(LI)*64 + (LJ)*16 + (LK)*4 + (LL)] = jk_launch<LI, LJ, LK, LL, double>; \
+#define JK_REG(LI, LJ, LK, LL)                                                       \
+    T->t64[(LI)*64 + (LJ)*16 + (LK)*4 + (LL)] = jk_launch<LI, LJ, LK, LL, double>;  \
+    T->b64[(LI)*64 + (LJ)*16 + (LK)*4 + (LL)] = jk_launch_batch<LI, LJ, LK, LL, double>; \
     JK_REG32(LI, LJ, LK, LL)

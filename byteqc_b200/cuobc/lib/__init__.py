@@ -58,6 +58,14 @@ _SIGNATURES = {
     'jk_int1e_cart': [ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
                       ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                       ctypes.c_void_p],
+    'jk_batch_create': [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p],
+    'jk_batch_destroy': [ctypes.c_void_p],
+    'jk_batch_build': [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                       ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                       ctypes.c_void_p],
+    'jk_batch_get_jk': [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                        ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
     'jk_last_error': [],
 }
 

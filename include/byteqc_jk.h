@@ -25,6 +25,7 @@ extern "C" {
 #define JK_ERR_ARG 3         /* invalid argument */
 
 typedef struct jk_basis jk_basis_t;
+typedef struct jk_batch jk_batch_t;
 
 typedef struct {
     double direct_scf_tol; /* density screen threshold (mf.direct_scf_tol)    */
@@ -113,6 +114,31 @@ int jk_build(jk_basis_t *basis, const double *dm, int n_dm, double *vj, double *
  */
 int jk_get_jk(jk_basis_t *basis, const double *coeff, int nao0, const double *dm0, int n_dm, double *vj0,
               double *vk0, const jk_opts_t *opts, void *stream);
+
+/*
+ * Batched builds over many molecules (one jk_basis each, same device).  No
+ * single reference counterpart: the reference builds one molecule at a time
+ * through the task loop of get_jk (cuobc/scf/hf.py:111-166); a batch runs
+ * the class quartets of all molecules that share a class (angular momenta
+ * and primitive counts) as one launch, with the same screening decisions as
+ * jk_build for each molecule.
+ */
+int jk_batch_create(jk_basis_t *const *bases, int nmol, jk_batch_t **out);
+int jk_batch_destroy(jk_batch_t *batch);
+
+/* Per molecule m: dms[m] device density in the working basis, vjs[m]/vks[m]
+ * device buffers accumulated as in jk_build (either array may be NULL).  The
+ * segment tables follow the pointers: a call with new pointers synchronises
+ * `stream` once to rebuild them; with the same pointers the call is fully
+ * asynchronous. */
+int jk_batch_build(jk_batch_t *batch, const double *const *dms, double *const *vjs, double *const *vks, int n_dm,
+                   const jk_opts_t *opts, void *stream);
+
+/* Full J/K of every molecule in its own basis (the jk_get_jk contract per
+ * molecule): coeffs[m] device (nao_m, nao0s[m]); dm0s[m], vj0s[m], vk0s[m]
+ * device (n_dm, nao0, nao0); vj0s/vk0s overwritten, either array may be NULL. */
+int jk_batch_get_jk(jk_batch_t *batch, const double *const *coeffs, const int *nao0s, const double *const *dm0s,
+                    double *const *vj0s, double *const *vk0s, int n_dm, const jk_opts_t *opts, void *stream);
 
 /* Rys nodes s = t^2 and weights of the product tables, evaluated on the
  * host (for checking the tables).  Returns JK_ERR_ARG for n outside 1..11. */
