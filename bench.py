@@ -48,6 +48,82 @@ def make_workload(name):
     return mol, dm
 
 
+def batch_workload(nmol=256, seed=4, basis='standin-6-31g*'):
+    """Seeded molecules of 3-60 atoms grown by a random walk (elements
+    C:N:O:H = 3:1:1:5), each with a D = 2 C C^T density."""
+    from byteqc_b200.gto import Mole, geom
+    rng = np.random.default_rng(seed)
+    mols, dms = [], []
+    for i in range(nmol):
+        natm = int(rng.integers(3, 61))
+        m = Mole(atom=geom.random_walk_molecule(natm, seed=seed * 100003 + i),
+                 basis=basis).build()
+        s = m.intor('int1e_ovlp')
+        mols.append(m)
+        dms.append(geom.scf_like_density(s, nocc=m.nelectron // 2, seed=i))
+    return mols, dms
+
+
+def bench_batch(args, torch, timed):
+    """Batched builds of the 256-molecule workload: per-molecule launches,
+    one batched pass, the batch in mixed precision, and both from a captured
+    CUDA graph.  Returns the 'batch' sub-object of the bench line."""
+    from byteqc_b200.cuobc.scf import hf
+    from byteqc_b200.cuobc.scf.batch import JKBatch
+    mols, dms = batch_workload(args.batch_mols)
+    t = time.perf_counter()
+    batch = JKBatch(mols)
+    torch.cuda.synchronize()
+    setup = time.perf_counter() - t
+    nbf = [m.nao for m in mols]
+    d_dms = [torch.as_tensor(d, device='cuda') for d in dms]
+
+    def per_molecule():
+        for m, d, o in zip(mols, d_dms, batch.opts):
+            hf.get_jk(m, d, vhfopt=o, out='device')
+
+    def batched(cut):
+        def f():
+            batch._run(1, True, True, batch._opts(True, None, cut))
+        return f
+    ref = batch.get_jk(d_dms, out='device')
+
+    def err_vs_ref():
+        got = batch._results(batch._graph[1] if batch._graph else
+                             [tuple(d.shape) for d in d_dms], True, True, 'device')
+        return max(max((a[0] - b[0]).abs().max().item(),
+                       (a[1] - b[1]).abs().max().item())
+                   for a, b in zip(ref, got))
+    batch._load(d_dms)
+    res = {}
+    for name, fn in (('per_molecule_fp64', per_molecule),
+                     ('batched_fp64', batched(0.)),
+                     ('batched_mixed', batched(args.fp32_cutoff))):
+        for _ in range(2):
+            fn()
+        ms = timed(fn, max(2, args.steps))
+        res[name] = {'ms': ms, 'builds_per_s': len(mols) * 1e3 / ms}
+        if name.startswith('batched'):
+            res[name]['max_abs_err_jk_vs_fp64'] = err_vs_ref()
+    # graph replays
+    for name, cut in (('graph_fp64', 0.), ('graph_mixed', args.fp32_cutoff)):
+        batch.capture(d_dms, fp32_cutoff=cut)
+        g = batch._graph[0]
+        for _ in range(2):
+            g.replay()
+        ms = timed(g.replay, max(2, args.steps))
+        res[name] = {'ms': ms, 'builds_per_s': len(mols) * 1e3 / ms}
+        res[name]['max_abs_err_jk_vs_fp64'] = err_vs_ref()
+    base = res['per_molecule_fp64']['builds_per_s']
+    return {'molecules': len(mols), 'basis': 'standin-6-31g*',
+            'nbf_min': min(nbf), 'nbf_max': max(nbf), 'nbf_mean': float(np.mean(nbf)),
+            'setup_s': setup, 'variants': res,
+            'speedup_graph_mixed_vs_per_molecule_fp64':
+                res['graph_mixed']['builds_per_s'] / base,
+            'speedup_graph_mixed_vs_graph_fp64':
+                res['graph_mixed']['builds_per_s'] / res['graph_fp64']['builds_per_s']}
+
+
 def ncart(l):
     return (l + 1) * (l + 2) // 2
 
@@ -184,6 +260,8 @@ def main():
     ap.add_argument('--workload', default='h2o32-tzvp', choices=sorted(WORKLOADS))
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--ref-sample-s', type=float, default=12.0)
+    ap.add_argument('--batch-mols', type=int, default=256,
+                    help='molecules of the batched workload (0: skip)')
     ap.add_argument('--fp32-cutoff', type=float, default=1e-6,
                     help='also time the mixed-precision build at this cutoff '
                          '(0: skip)')
@@ -347,6 +425,8 @@ def main():
                 'd2h_bytes_per_step': int(2 * dm.nbytes)},
         'clocks': clk.summary(),
     }
+    if args.batch_mols > 0:
+        line['batch'] = bench_batch(args, torch, timed)
     if ms_mixed is not None:
         line['mixed'] = {'fp32_cutoff': args.fp32_cutoff,
                          'value': world * 1e3 / ms_mixed, 'unit': 'builds/s',
