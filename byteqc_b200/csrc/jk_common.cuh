@@ -327,6 +327,7 @@ struct JKSeg {
     const int* pair2bra;
     const int* pair2ket;
     const double* a12;
+    const double* ia12;  // 1 / a12
     const double* e12;
     const double* x12;
     const double* y12;

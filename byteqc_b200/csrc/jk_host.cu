@@ -112,6 +112,9 @@ __global__ void jk_qcond_kernel(const int* __restrict__ pi, const int* __restric
                     pr.A = A;
                     pr.B = B;
                     pr.AB = A + B;
+                    pr.iA = 1. / A;
+                    pr.iB = 1. / B;
+                    pr.iAB = 1. / pr.AB;
                     for (int d = 0; d < 3; d++) {
                         pr.P[d] = P[d];
                         pr.Q[d] = (ai[kp] * ri[d] + aj[lp] * rj[d]) / B;
@@ -526,8 +529,9 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
         b->h_prim_locs.push_back((int)npp);
     }
     b->nprim_total = npp;
-    std::vector<double> prim(5 * (size_t)(npp ? npp : 1));
+    std::vector<double> prim(6 * (size_t)(npp ? npp : 1));
     double *a12 = prim.data(), *e12 = a12 + npp, *x12 = e12 + npp, *y12 = x12 + npp, *z12 = y12 + npp;
+    double* ia12 = z12 + npp;
     {
         long long off = 0;
         for (size_t p = 0; p < b->h_pair2bra.size(); p++) {
@@ -547,6 +551,7 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
                 for (int jp = 0; jp < npj; jp++, off++) {
                     double aij = ai[ip] + aj[jp];
                     a12[off] = aij;
+                    ia12[off] = 1. / aij;
                     e12[off] = norm * ci[ip] * cj[jp] * exp(-r2 * ai[ip] * aj[jp] / aij);
                     if (ish == jsh) e12[off] *= b->diag_fac;
                     x12[off] = (ai[ip] * ri[0] + aj[jp] * rj[0]) / aij;
@@ -673,6 +678,7 @@ static void fill_seg(const jk_basis* b, int cp_ij, int cp_kl, const long long* q
     s->x12 = b->d_prim + 2 * n;
     s->y12 = b->d_prim + 3 * n;
     s->z12 = b->d_prim + 4 * n;
+    s->ia12 = b->d_prim + 5 * n;
     s->bas_x = b->d_bas_x;
     s->nbas = b->nbas;
     s->ao_loc = b->d_ao_loc;

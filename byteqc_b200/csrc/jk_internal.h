@@ -54,7 +54,7 @@ struct jk_basis {
     int *d_atm = nullptr, *d_bas = nullptr, *d_ao_loc = nullptr, *d_group_ao = nullptr;
     double *d_env = nullptr, *d_bas_x = nullptr, *d_qcond = nullptr;
     int *d_pair2bra = nullptr, *d_pair2ket = nullptr;
-    double *d_log_q = nullptr, *d_log_q_raw = nullptr, *d_prim = nullptr;  // prim: a12|e12|x12|y12|z12
+    double *d_log_q = nullptr, *d_log_q_raw = nullptr, *d_prim = nullptr;  // prim: a12|e12|x12|y12|z12|1/a12
     long long nprim_total = 0;
     JKScreenCQ* d_cq = nullptr;
     long long *d_qoff = nullptr, *d_task0 = nullptr;

@@ -140,6 +140,7 @@ struct JKSegTable {
 // prefactors of one primitive quartet
 struct JKPrim {
     double x, A, B, AB, sy;  // Boys argument, exponent sums, y seed
+    double iA, iB, iAB;      // 1/A, 1/B, 1/(A+B)
     double P[3], Q[3];
 };
 
@@ -153,11 +154,14 @@ __device__ __forceinline__ JKPrim jk_prim(const JKSeg& sg, int pij, int pkl) {
     p.Q[0] = __ldg(sg.x12 + pkl);
     p.Q[1] = __ldg(sg.y12 + pkl);
     p.Q[2] = __ldg(sg.z12 + pkl);
+    p.iA = __ldg(sg.ia12 + pij);
+    p.iB = __ldg(sg.ia12 + pkl);
     p.AB = p.A + p.B;
-    double rho = p.A * p.B / p.AB;
+    p.iAB = 1. / p.AB;
+    double rho = p.A * p.B * p.iAB;
     double dx = p.P[0] - p.Q[0], dy = p.P[1] - p.Q[1], dz = p.P[2] - p.Q[2];
     p.x = rho * (dx * dx + dy * dy + dz * dz);
-    p.sy = __ldg(sg.e12 + pij) * __ldg(sg.e12 + pkl) / (sqrt(p.AB) * p.A * p.B);
+    p.sy = __ldg(sg.e12 + pij) * __ldg(sg.e12 + pkl) * p.iA * p.iB * sqrt(p.iAB);
     return p;
 }
 
@@ -167,10 +171,11 @@ __device__ __forceinline__ void jk_unit(const JKPrim& p, double s, double w, int
                                         const double* rj, const double* rk, const double* rl, OutT* out) {
     // select by d without dynamic indexing (keeps everything in registers)
 #define JK_PICK(a) (d == 0 ? (a)[0] : (d == 1 ? (a)[1] : (a)[2]))
-    double bs = p.B * s / p.AB, as = p.A * s / p.AB;
-    double b00 = 0.5 * s / p.AB;
-    double b10 = 0.5 / p.A * (1. - bs);
-    double b01 = 0.5 / p.B * (1. - as);
+    double siAB = s * p.iAB;
+    double bs = p.B * siAB, as = p.A * siAB;
+    double b00 = 0.5 * siAB;
+    double b10 = 0.5 * p.iA * (1. - bs);
+    double b01 = 0.5 * p.iB * (1. - as);
     double Pd = JK_PICK(p.P), Qd = JK_PICK(p.Q);
     double Rid = JK_PICK(ri), Rjd = JK_PICK(rj), Rkd = JK_PICK(rk), Rld = JK_PICK(rl);
 #undef JK_PICK
