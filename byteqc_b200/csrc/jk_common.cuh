@@ -200,6 +200,100 @@ __device__ __forceinline__ void rys_root(const double* __restrict__ rys_coef, do
 }
 
 // ---------------------------------------------------------------------------
+// Single-precision nodes and weights for the FP32 quartets of the mixed mode
+// at low order (n <= JK_F32_ROOTS): the Boys function in float for n = 1, the
+// same Chebyshev tables rounded to float for n = 2, 3.  Higher orders keep
+// the double evaluation above.  Same shared-memory layout as the double copy
+// (the stride is odd in floats too).
+// ---------------------------------------------------------------------------
+#define JK_F32_ROOTS 3
+
+template <int N>
+__device__ __forceinline__ void rys_table_to_smem_f(const double* __restrict__ g, float* __restrict__ tab) {
+    using S = RysS<N>;
+    if (N == 1) return;
+    const double* src = g + rys_off_c(N);
+    for (int e = threadIdx.x; e < S::NINT * S::NS * RYS_NC; e += blockDim.x) {
+        int m = e / (S::NS * RYS_NC);
+        int rem = e - m * (S::NS * RYS_NC);
+        int f = rem / RYS_NC, k = rem - f * RYS_NC;
+        tab[m * S::STRIDE + k * S::NS + f] = (float)__ldg(src + e);
+    }
+    for (int r = threadIdx.x; r < N; r += blockDim.x) {
+        tab[S::HERM + r] = (float)rys_herm_r[N * (N - 1) / 2 + r];
+        tab[S::HERM + N + r] = (float)rys_herm_w[N * (N - 1) / 2 + r];
+    }
+}
+
+// F0 and F1 in float: the series below x = 0.75 (12 terms, truncation below
+// 1e-10), erf/exp above
+__device__ __forceinline__ void boys01_f(float x, float& f0, float& f1) {
+    if (x < 0.75f) {
+        float a0 = 0.f, a1 = 0.f;
+        double fk = 1.;
+        float c0[12], c1[12];
+#pragma unroll
+        for (int k = 0; k < 12; k++) {
+            if (k) fk *= k;
+            c0[k] = (float)(((k & 1) ? -1. : 1.) / (fk * (2 * k + 1)));
+            c1[k] = (float)(((k & 1) ? -1. : 1.) / (fk * (2 * k + 3)));
+        }
+#pragma unroll
+        for (int k = 11; k >= 0; k--) {
+            a0 = fmaf(a0, x, c0[k]);
+            a1 = fmaf(a1, x, c1[k]);
+        }
+        f0 = a0;
+        f1 = a1;
+    } else {
+        float rsx = rsqrtf(x);
+        f0 = 0.886226925f * erff(x * rsx) * rsx;  // sqrt(pi)/2 erf(sqrt x)/sqrt x
+        f1 = (f0 - expf(-x)) * (0.5f * rsx * rsx);
+    }
+}
+
+template <int N>
+__device__ __forceinline__ void rys_roots_all_f(const float* __restrict__ tab, float x, float* s, float* w) {
+    using S = RysS<N>;
+    if (N == 1) {
+        float f0, f1;
+        boys01_f(x, f0, f1);
+        w[0] = f0;
+        s[0] = __fdividef(f1, f0);
+        return;
+    }
+    if (x >= (float)S::XMAX) {
+        float srx = rsqrtf(x), rx = srx * srx;
+#pragma unroll
+        for (int r = 0; r < N; r++) {
+            s[r] = tab[S::HERM + r] * rx;
+            w[r] = tab[S::HERM + N + r] * srx;
+        }
+        return;
+    }
+    int m = (int)(x * 0.5f);
+    float t = x - (float)(2 * m + 1), t2 = t + t;
+    const float* c = tab + m * S::STRIDE;
+    float b1[S::NS], b2[S::NS];
+#pragma unroll
+    for (int f = 0; f < S::NS; f++) b1[f] = b2[f] = 0.f;
+#pragma unroll
+    for (int k = RYS_NC - 1; k >= 1; k--) {
+#pragma unroll
+        for (int f = 0; f < S::NS; f++) {
+            float b0 = fmaf(t2, b1[f], c[k * S::NS + f] - b2[f]);
+            b2[f] = b1[f];
+            b1[f] = b0;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < N; r++) {
+        s[r] = fmaf(t, b1[r], c[r] - b2[r]);
+        w[r] = fmaf(t, b1[N + r], c[N + r] - b2[N + r]);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Compile-time class description for (li lj | lk ll), li >= lj, lk >= ll.
 // ---------------------------------------------------------------------------
 __host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
@@ -332,6 +426,10 @@ struct JKSeg {
     const double* x12;
     const double* y12;
     const double* z12;
+    // FP32 copy of the primitive pairs for the FP32 quartets of the mixed
+    // mode, SoA of npf floats each: a12 | 1/a12 | e12/a12 | P - R_bra (x, y, z)
+    const float* pf;
+    long long npf;
     const double* bas_x;  // shell centres, SoA x[nbas], y[nbas], z[nbas]
     int nbas;
     const int* ao_loc;
@@ -345,3 +443,4 @@ typedef cudaError_t (*jk_launch_fn)(const JKSeg& seg, const long long* task0, lo
                                     cudaStream_t st);
 typedef cudaError_t (*jk_launch_batch_fn)(const JKSeg* segs, const long long* segt, int nseg, long long max_tasks,
                                           int nsm, cudaStream_t st);
+

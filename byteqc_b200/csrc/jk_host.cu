@@ -233,6 +233,12 @@ __device__ __forceinline__ void jk_block_scan2(long long a, long long b, long lo
     __syncthreads();
 }
 
+// max over the six group pairs of a class quartet of the condensed density
+__device__ __forceinline__ double jk_cq_sub(const double* c, int ngroups, int gi, int gj, int gk, int gl) {
+    return fmax(fmax(fmax(c[gi * ngroups + gj], c[gk * ngroups + gl]), fmax(c[gi * ngroups + gk], c[gj * ngroups + gk])),
+                fmax(c[gi * ngroups + gl], c[gj * ngroups + gl]));
+}
+
 // One block (256 threads) per class quartet.  Reproduces the reference's
 // screening decision per contracted quartet (cuobc/scf/hf.py:136-145,
 // 567-578 and cuobc/lib/gvhf/nr_jk_driver.cu:252-280):
@@ -254,9 +260,7 @@ __global__ void jk_screen_kernel(const JKScreenCQ* __restrict__ cqs, double tol,
     int* klb = cq.klb;
     const double* c = cq.dm_cond;
     const int ngroups = cq.ngroups;
-    double sub = fmax(fmax(fmax(c[cq.gi * ngroups + cq.gj], c[cq.gk * ngroups + cq.gl]),
-                           fmax(c[cq.gi * ngroups + cq.gk], c[cq.gj * ngroups + cq.gk])),
-                      fmax(c[cq.gi * ngroups + cq.gl], c[cq.gj * ngroups + cq.gl]));
+    const double sub = jk_cq_sub(c, ngroups, cq.gi, cq.gj, cq.gk, cq.gl);
     bool skip = prescreen && sub < tol;
     double cutoff = tol / sub;
     double scale = nbins / log(fmin(cutoff, 0.1));
@@ -354,6 +358,7 @@ static void free_basis(jk_basis* b) {
     cudaFree(b->d_task032);
     cudaFree(b->d_klb);
     cudaFree(b->d_prim);
+    cudaFree(b->d_primf);
     cudaFree(b->d_cq);
     cudaFree(b->d_qoff);
     cudaFree(b->d_task0);
@@ -532,6 +537,10 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
     std::vector<double> prim(6 * (size_t)(npp ? npp : 1));
     double *a12 = prim.data(), *e12 = a12 + npp, *x12 = e12 + npp, *y12 = x12 + npp, *z12 = y12 + npp;
     double* ia12 = z12 + npp;
+    // single-precision copy for the FP32 quartets of the mixed mode; the
+    // product centre is stored relative to the bra shell's centre so that
+    // the small differences P - R_i keep their relative precision
+    std::vector<float> primf(6 * (size_t)(npp ? npp : 1));
     {
         long long off = 0;
         for (size_t p = 0; p < b->h_pair2bra.size(); p++) {
@@ -557,10 +566,18 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
                     x12[off] = (ai[ip] * ri[0] + aj[jp] * rj[0]) / aij;
                     y12[off] = (ai[ip] * ri[1] + aj[jp] * rj[1]) / aij;
                     z12[off] = (ai[ip] * ri[2] + aj[jp] * rj[2]) / aij;
+                    primf[off] = (float)aij;
+                    primf[npp + off] = (float)(1. / aij);
+                    primf[2 * npp + off] = (float)(e12[off] / aij);
+                    // P - R_i = aj (R_j - R_i) / (ai + aj)
+                    primf[3 * npp + off] = (float)(aj[jp] * (rj[0] - ri[0]) / aij);
+                    primf[4 * npp + off] = (float)(aj[jp] * (rj[1] - ri[1]) / aij);
+                    primf[5 * npp + off] = (float)(aj[jp] * (rj[2] - ri[2]) / aij);
                 }
         }
     }
     CUDA_TRY(upload(&b->d_prim, prim.data(), prim.size()));
+    CUDA_TRY(upload(&b->d_primf, primf.data(), primf.size()));
     CUDA_TRY(upload(&b->d_pair2bra, b->h_pair2bra.data(), b->h_pair2bra.size()));
     CUDA_TRY(upload(&b->d_pair2ket, b->h_pair2ket.data(), b->h_pair2ket.size()));
     CUDA_TRY(upload(&b->d_log_q, b->h_log_q.data(), b->h_log_q.size()));
@@ -679,6 +696,8 @@ static void fill_seg(const jk_basis* b, int cp_ij, int cp_kl, const long long* q
     s->y12 = b->d_prim + 3 * n;
     s->z12 = b->d_prim + 4 * n;
     s->ia12 = b->d_prim + 5 * n;
+    s->pf = b->d_primf;
+    s->npf = n;
     s->bas_x = b->d_bas_x;
     s->nbas = b->nbas;
     s->ao_loc = b->d_ao_loc;
@@ -932,15 +951,26 @@ extern "C" int jk_fma_peak(int fp32, double* tflops) {
 // device evaluation of the Rys tables at a batch of points, through the
 // paths the kernels use: mode 0 all roots from the shared-memory copy (thread
 // kernels), 1 one root at a time from it (team kernels), 2 one root from the
-// global table (setup kernels)
+// global table (setup kernels), 3 all roots in single precision (the FP32
+// quartets of the mixed mode, n <= JK_F32_ROOTS)
 template <int N>
 __global__ void jk_rys_eval_kernel(const double* rys, const double* x, int count, double* s, double* w, int mode) {
     extern __shared__ __align__(16) double tab[];
-    rys_table_to_smem<N>(rys, tab);
+    if (mode == 3) rys_table_to_smem_f<N>(rys, reinterpret_cast<float*>(tab));
+    else rys_table_to_smem<N>(rys, tab);
     __syncthreads();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
-    if (mode == 0) {
+    if (mode == 3) {
+        if constexpr (N <= JK_F32_ROOTS) {
+            float rs[N], rw[N];
+            rys_roots_all_f<N>(reinterpret_cast<const float*>(tab), (float)x[i], rs, rw);
+            for (int r = 0; r < N; r++) {
+                s[i * N + r] = rs[r];
+                w[i * N + r] = rw[r];
+            }
+        }
+    } else if (mode == 0) {
         double rs[N], rw[N];
         rys_roots_all<N>(tab, x[i], rs, rw);
         for (int r = 0; r < N; r++) {
@@ -966,7 +996,8 @@ static cudaError_t rys_eval_launch(const double* rys, const double* x, int count
 }
 
 extern "C" int jk_rys_roots_device(int n, const double* x, int count, double* s, double* w, int mode, void* stream) {
-    if (n < 1 || n > 11 || !x || !s || !w || count < 0 || mode < 0 || mode > 2)
+    if (n < 1 || n > 11 || !x || !s || !w || count < 0 || mode < 0 || mode > 3 ||
+        (mode == 3 && n > JK_F32_ROOTS))
         return set_err(JK_ERR_ARG, "jk_rys_roots_device: bad args");
     if (count == 0) return JK_OK;
     const double* rys;

@@ -55,6 +55,7 @@ struct jk_basis {
     double *d_env = nullptr, *d_bas_x = nullptr, *d_qcond = nullptr;
     int *d_pair2bra = nullptr, *d_pair2ket = nullptr;
     double *d_log_q = nullptr, *d_log_q_raw = nullptr, *d_prim = nullptr;  // prim: a12|e12|x12|y12|z12|1/a12
+    float* d_primf = nullptr;  // FP32 path: a12|1/a12|e12/a12|P-R_bra (x, y, z)
     long long nprim_total = 0;
     JKScreenCQ* d_cq = nullptr;
     long long *d_qoff = nullptr, *d_task0 = nullptr;

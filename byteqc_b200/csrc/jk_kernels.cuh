@@ -178,13 +178,69 @@ __device__ __forceinline__ void jk_unit(const JKPrim& p, double s, double w, int
     double b01 = 0.5 * p.iB * (1. - as);
     double Pd = JK_PICK(p.P), Qd = JK_PICK(p.Q);
     double Rid = JK_PICK(ri), Rjd = JK_PICK(rj), Rkd = JK_PICK(rk), Rld = JK_PICK(rl);
-#undef JK_PICK
     double pq = Pd - Qd;
     double c00 = (Pd - Rid) - bs * pq;
     double c0p = (Qd - Rkd) + as * pq;
     double seed = d == 0 ? norm : (d == 1 ? p.sy : w);
     rys_2d<R, C>((R)seed, (R)c00, (R)c0p, (R)b10, (R)b01, (R)b00, (R)(Rid - Rjd), (R)(Rkd - Rld), out);
 }
+
+// ---------------------------------------------------------------------------
+// FP32 quartets of the mixed mode at low order: the primitive prefactors,
+// the Boys function / Rys nodes and the recursion all in float.  Pair data
+// comes from the float copy (JKSeg::pf); P - Q is formed from the small
+// differences P - R_i, Q - R_k and the centre difference R_i - R_k (computed
+// in double once per contracted quartet) so that it keeps its relative
+// precision.
+// ---------------------------------------------------------------------------
+struct JKPrimF {
+    float x, A, B, iA, iB, iAB, sy;
+    float PA[3], QC[3], PQ[3];
+};
+
+__device__ __forceinline__ JKPrimF jk_prim_f(const JKSeg& sg, int pij, int pkl, const float* ac) {
+    const float* f = sg.pf;
+    const long long n = sg.npf;
+    JKPrimF p;
+    p.A = __ldg(f + pij);
+    p.B = __ldg(f + pkl);
+    p.iA = __ldg(f + n + pij);
+    p.iB = __ldg(f + n + pkl);
+    const float E = __ldg(f + 2 * n + pij) * __ldg(f + 2 * n + pkl);
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        p.PA[d] = __ldg(f + (3 + d) * n + pij);
+        p.QC[d] = __ldg(f + (3 + d) * n + pkl);
+        p.PQ[d] = (p.PA[d] - p.QC[d]) + ac[d];
+    }
+    const float rs = rsqrtf(p.A + p.B);
+    p.iAB = rs * rs;
+    p.x = p.A * p.B * p.iAB * (p.PQ[0] * p.PQ[0] + p.PQ[1] * p.PQ[1] + p.PQ[2] * p.PQ[2]);
+    p.sy = E * rs;  // e12 e12' / (A B sqrt(A + B))
+    return p;
+}
+
+template <class C, typename OutT>
+__device__ __forceinline__ void jk_unit_f(const JKPrimF& p, float s, float w, int d, float norm, const float* dij,
+                                          const float* dkl, OutT* out) {
+    float siAB = s * p.iAB;
+    float bs = p.B * siAB, as = p.A * siAB;
+    float b00 = 0.5f * siAB;
+    float b10 = 0.5f * p.iA * (1.f - bs);
+    float b01 = 0.5f * p.iB * (1.f - as);
+    float pq = JK_PICK(p.PQ);
+    float c00 = JK_PICK(p.PA) - bs * pq;
+    float c0p = JK_PICK(p.QC) + as * pq;
+    float seed = d == 0 ? norm : (d == 1 ? p.sy : w);
+    rys_2d<float, C>(seed, c00, c0p, b10, b01, b00, JK_PICK(dij), JK_PICK(dkl), out);
+}
+#undef JK_PICK
+
+// FP32 primitive path for this class and arithmetic type
+template <class C, typename R>
+struct JKF32Prim {
+    static constexpr bool value = sizeof(R) == 4 && C::NROOTS <= JK_F32_ROOTS;
+};
 
 __device__ __forceinline__ void load_center(const JKSeg& sg, int sh, double* r) {
     r[0] = __ldg(sg.bas_x + sh);
@@ -201,51 +257,47 @@ __device__ __forceinline__ void load_center(const JKSeg& sg, int sh, double* r) 
 // run NPASS passes over the primitive quartets (the 2D blocks are rebuilt
 // per pass, the accumulators of one pass only are live).
 // ===========================================================================
-template <class C, typename R, int CI0, int CI1>
-__device__ __forceinline__ void jk_thread_pass(const JKSeg& sg, const JKQuartet& q, const double* __restrict__ tab,
-                                               const double* ri, const double* rj, const double* rk,
-                                               const double* rl) {
-    constexpr int NR = C::NROOTS;
-    constexpr int NI = CI1 - CI0;
-    constexpr int NA = NI * C::NFJ * C::NFK * C::NFL;
-    R acc[NA];
-#pragma unroll
-    for (int e = 0; e < NA; e++) acc[e] = R(0);
-    for (int ip = 0; ip < sg.nprim_ij; ip++)
-        for (int kp = 0; kp < sg.nprim_kl; kp++) {
-            JKPrim p = jk_prim(sg, q.prim_ij + ip, q.prim_kl + kp);
-            double rs[NR], rw[NR];
-            rys_roots_all<NR>(tab, p.x, rs, rw);
-#pragma unroll
-            for (int r = 0; r < NR; r++) {
-                const double s = rs[r], w = rw[r];
-                R Ix[C::GS], Iy[C::GS], Iz[C::GS];
-                jk_unit<C, R>(p, s, w, 0, q.norm, ri, rj, rk, rl, Ix);
-                jk_unit<C, R>(p, s, w, 1, q.norm, ri, rj, rk, rl, Iy);
-                jk_unit<C, R>(p, s, w, 2, q.norm, ri, rj, rk, rl, Iz);
-#pragma unroll
-                for (int i = 0; i < NI; i++)
-#pragma unroll
-                    for (int j = 0; j < C::NFJ; j++)
-#pragma unroll
-                        for (int k = 0; k < C::NFK; k++)
-#pragma unroll
-                            for (int l = 0; l < C::NFL; l++) {
-                                int ox = cart_lx(C::LI, CI0 + i) * C::SI + cart_lx(C::LJ, j) * C::SJ +
-                                         cart_lx(C::LK, k) * C::SK + cart_lx(C::LL, l);
-                                int oy = cart_ly(C::LI, CI0 + i) * C::SI + cart_ly(C::LJ, j) * C::SJ +
-                                         cart_ly(C::LK, k) * C::SK + cart_ly(C::LL, l);
-                                int oz = cart_lz(C::LI, CI0 + i) * C::SI + cart_lz(C::LJ, j) * C::SJ +
-                                         cart_lz(C::LK, k) * C::SK + cart_lz(C::LL, l);
-                                acc[((i * C::NFJ + j) * C::NFK + k) * C::NFL + l] += Ix[ox] * Iy[oy] * Iz[oz];
-                            }
-            }
-        }
+// ---------------------------------------------------------------------------
+// Digestion of one quartet's Cartesian block (bra components ci in
+// [CI0, CI0 + NI)) into J and K through a sink:
+//   J_ij += (ij|kl) D_kl, J_kl += (ij|kl) D_ij,
+//   K_ik += (ij|kl) D_jl, K_il += (ij|kl) D_jk, K_jk += (ij|kl) D_il,
+//   K_jl += (ij|kl) D_ik
+// (cuobc/lib/gvhf/contract_jk.cu:225-316).  JKSinkGlobal adds every element
+// to the output buffers with one global atomic, element (a, b) at a + nao*b;
+// JKSinkSmem adds into the shared-memory blocks of a tile.
+// ---------------------------------------------------------------------------
+struct JKSinkGlobal {
+    double* vj;
+    double* vk;
+    int nao;
+    size_t nn;
+    __device__ __forceinline__ void jij(int idm, int a, int b, double v) const {
+        atomicAdd(vj + idm * nn + a + (size_t)nao * b, v);
+    }
+    __device__ __forceinline__ void jkl(int idm, int a, int b, double v) const {
+        atomicAdd(vj + idm * nn + a + (size_t)nao * b, v);
+    }
+    __device__ __forceinline__ void kik(int idm, int a, int b, double v) const {
+        atomicAdd(vk + idm * nn + a + (size_t)nao * b, v);
+    }
+    __device__ __forceinline__ void kil(int idm, int a, int b, double v) const { kik(idm, a, b, v); }
+    __device__ __forceinline__ void kjk(int idm, int a, int b, double v) const { kik(idm, a, b, v); }
+    __device__ __forceinline__ void kjl(int idm, int a, int b, double v) const { kik(idm, a, b, v); }
+};
+
+__device__ __forceinline__ JKSinkGlobal jk_sink_global(const JKSeg& sg) {
+    return JKSinkGlobal{sg.vj, sg.vk, sg.nao, (size_t)sg.nao * sg.nao};
+}
+
+template <class C, typename R, int NI, class Sink>
+__device__ __forceinline__ void jk_thread_digest(const JKSeg& sg, const JKQuartet& q, int CI0, const R* acc,
+                                                 const Sink& sink) {
     const int nao = sg.nao;
     const int i0 = __ldg(sg.ao_loc + q.ish) + CI0, j0 = __ldg(sg.ao_loc + q.jsh);
     const int k0 = __ldg(sg.ao_loc + q.ksh), l0 = __ldg(sg.ao_loc + q.lsh);
     // the lanes of a warp usually share the ij pair (consecutive kl of one
-    // row): then the J_ij block is summed over the warp before its atomics
+    // row): then the J_ij block is summed over the warp before it is added
     const unsigned am = __activemask();
     bool wsame = false;
     if (am == 0xffffffffu) {
@@ -256,7 +308,6 @@ __device__ __forceinline__ void jk_thread_pass(const JKSeg& sg, const JKQuartet&
     for (int idm = 0; idm < sg.n_dm; idm++) {
         const double* D = sg.dm + (size_t)idm * nao * nao;
         if (sg.vj) {
-            double* V = sg.vj + (size_t)idm * nao * nao;
 #pragma unroll
             for (int i = 0; i < NI; i++)
 #pragma unroll
@@ -269,9 +320,9 @@ __device__ __forceinline__ void jk_thread_pass(const JKSeg& sg, const JKQuartet&
                     if (wsame) {
 #pragma unroll
                         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                        if ((threadIdx.x & 31) == 0) atomicAdd(V + (i0 + i) + (size_t)nao * (j0 + j), v);
+                        if ((threadIdx.x & 31) == 0) sink.jij(idm, i0 + i, j0 + j, v);
                     } else {
-                        atomicAdd(V + (i0 + i) + (size_t)nao * (j0 + j), v);
+                        sink.jij(idm, i0 + i, j0 + j, v);
                     }
                 }
 #pragma unroll
@@ -283,11 +334,10 @@ __device__ __forceinline__ void jk_thread_pass(const JKSeg& sg, const JKQuartet&
                     for (int i = 0; i < NI; i++)
 #pragma unroll
                         for (int j = 0; j < C::NFJ; j++) v += ACC(i, j, k, l) * DM(i0 + i, j0 + j);
-                    atomicAdd(V + (k0 + k) + (size_t)nao * (l0 + l), v);
+                    sink.jkl(idm, k0 + k, l0 + l, v);
                 }
         }
         if (sg.vk) {
-            double* V = sg.vk + (size_t)idm * nao * nao;
 #pragma unroll
             for (int i = 0; i < NI; i++)
 #pragma unroll
@@ -296,8 +346,8 @@ __device__ __forceinline__ void jk_thread_pass(const JKSeg& sg, const JKQuartet&
 #pragma unroll
                     for (int j = 0; j < C::NFJ; j++)
 #pragma unroll
-                        for (int l = 0; l < C::NFL; l++) v += ACC(i, j, k, l) * DM(j0 + j, l0 + l);
-                    atomicAdd(V + (i0 + i) + (size_t)nao * (k0 + k), v);
+                        for (int l = 0; l < C::NFL; l++) v += ACC(i, j, k, l) * DM(l0 + l, j0 + j);
+                    sink.kik(idm, i0 + i, k0 + k, v);
                 }
 #pragma unroll
             for (int i = 0; i < NI; i++)
@@ -307,8 +357,8 @@ __device__ __forceinline__ void jk_thread_pass(const JKSeg& sg, const JKQuartet&
 #pragma unroll
                     for (int j = 0; j < C::NFJ; j++)
 #pragma unroll
-                        for (int k = 0; k < C::NFK; k++) v += ACC(i, j, k, l) * DM(j0 + j, k0 + k);
-                    atomicAdd(V + (i0 + i) + (size_t)nao * (l0 + l), v);
+                        for (int k = 0; k < C::NFK; k++) v += ACC(i, j, k, l) * DM(k0 + k, j0 + j);
+                    sink.kil(idm, i0 + i, l0 + l, v);
                 }
 #pragma unroll
             for (int j = 0; j < C::NFJ; j++)
@@ -318,8 +368,8 @@ __device__ __forceinline__ void jk_thread_pass(const JKSeg& sg, const JKQuartet&
 #pragma unroll
                     for (int i = 0; i < NI; i++)
 #pragma unroll
-                        for (int l = 0; l < C::NFL; l++) v += ACC(i, j, k, l) * DM(i0 + i, l0 + l);
-                    atomicAdd(V + (j0 + j) + (size_t)nao * (k0 + k), v);
+                        for (int l = 0; l < C::NFL; l++) v += ACC(i, j, k, l) * DM(l0 + l, i0 + i);
+                    sink.kjk(idm, j0 + j, k0 + k, v);
                 }
 #pragma unroll
             for (int j = 0; j < C::NFJ; j++)
@@ -329,39 +379,119 @@ __device__ __forceinline__ void jk_thread_pass(const JKSeg& sg, const JKQuartet&
 #pragma unroll
                     for (int i = 0; i < NI; i++)
 #pragma unroll
-                        for (int k = 0; k < C::NFK; k++) v += ACC(i, j, k, l) * DM(i0 + i, k0 + k);
-                    atomicAdd(V + (j0 + j) + (size_t)nao * (l0 + l), v);
+                        for (int k = 0; k < C::NFK; k++) v += ACC(i, j, k, l) * DM(k0 + k, i0 + i);
+                    sink.kjl(idm, j0 + j, l0 + l, v);
                 }
         }
     }
 #undef ACC
 }
 
-template <class C, typename R, int PASS>
+// acc[i][j][k][l] += Ix Iy Iz for the bra components ci in [CI0, CI0 + NI)
+template <class C, typename R, int CI0, int NI>
+__device__ __forceinline__ void jk_thread_products(R* acc, const R* Ix, const R* Iy, const R* Iz) {
+#pragma unroll
+    for (int i = 0; i < NI; i++)
+#pragma unroll
+        for (int j = 0; j < C::NFJ; j++)
+#pragma unroll
+            for (int k = 0; k < C::NFK; k++)
+#pragma unroll
+                for (int l = 0; l < C::NFL; l++) {
+                    int ox = cart_lx(C::LI, CI0 + i) * C::SI + cart_lx(C::LJ, j) * C::SJ + cart_lx(C::LK, k) * C::SK +
+                             cart_lx(C::LL, l);
+                    int oy = cart_ly(C::LI, CI0 + i) * C::SI + cart_ly(C::LJ, j) * C::SJ + cart_ly(C::LK, k) * C::SK +
+                             cart_ly(C::LL, l);
+                    int oz = cart_lz(C::LI, CI0 + i) * C::SI + cart_lz(C::LJ, j) * C::SJ + cart_lz(C::LK, k) * C::SK +
+                             cart_lz(C::LL, l);
+                    acc[((i * C::NFJ + j) * C::NFK + k) * C::NFL + l] += Ix[ox] * Iy[oy] * Iz[oz];
+                }
+}
+
+template <class C, typename R, int CI0, int CI1, class Sink>
+__device__ __forceinline__ void jk_thread_pass(const JKSeg& sg, const JKQuartet& q, const double* __restrict__ tab,
+                                               const double* ri, const double* rj, const double* rk,
+                                               const double* rl, const Sink& sink) {
+    constexpr int NR = C::NROOTS;
+    constexpr int NI = CI1 - CI0;
+    constexpr int NA = NI * C::NFJ * C::NFK * C::NFL;
+    R acc[NA];
+#pragma unroll
+    for (int e = 0; e < NA; e++) acc[e] = R(0);
+    if constexpr (JKF32Prim<C, R>::value) {
+        const float* tabf = reinterpret_cast<const float*>(tab);
+        float dij[3], dkl[3], ac[3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            dij[d] = (float)(ri[d] - rj[d]);
+            dkl[d] = (float)(rk[d] - rl[d]);
+            ac[d] = (float)(ri[d] - rk[d]);
+        }
+        const float normf = (float)q.norm;
+        for (int ip = 0; ip < sg.nprim_ij; ip++)
+            for (int kp = 0; kp < sg.nprim_kl; kp++) {
+                JKPrimF p = jk_prim_f(sg, q.prim_ij + ip, q.prim_kl + kp, ac);
+                float rs[NR], rw[NR];
+                rys_roots_all_f<NR>(tabf, p.x, rs, rw);
+#pragma unroll
+                for (int r = 0; r < NR; r++) {
+                    float Ix[C::GS], Iy[C::GS], Iz[C::GS];
+                    jk_unit_f<C>(p, rs[r], rw[r], 0, normf, dij, dkl, Ix);
+                    jk_unit_f<C>(p, rs[r], rw[r], 1, normf, dij, dkl, Iy);
+                    jk_unit_f<C>(p, rs[r], rw[r], 2, normf, dij, dkl, Iz);
+                    jk_thread_products<C, R, CI0, NI>(acc, Ix, Iy, Iz);
+                }
+            }
+    } else {
+        for (int ip = 0; ip < sg.nprim_ij; ip++)
+            for (int kp = 0; kp < sg.nprim_kl; kp++) {
+                JKPrim p = jk_prim(sg, q.prim_ij + ip, q.prim_kl + kp);
+                double rs[NR], rw[NR];
+                rys_roots_all<NR>(tab, p.x, rs, rw);
+#pragma unroll
+                for (int r = 0; r < NR; r++) {
+                    const double s = rs[r], w = rw[r];
+                    R Ix[C::GS], Iy[C::GS], Iz[C::GS];
+                    jk_unit<C, R>(p, s, w, 0, q.norm, ri, rj, rk, rl, Ix);
+                    jk_unit<C, R>(p, s, w, 1, q.norm, ri, rj, rk, rl, Iy);
+                    jk_unit<C, R>(p, s, w, 2, q.norm, ri, rj, rk, rl, Iz);
+                    jk_thread_products<C, R, CI0, NI>(acc, Ix, Iy, Iz);
+                }
+            }
+    }
+    jk_thread_digest<C, R, NI>(sg, q, CI0, acc, sink);
+}
+
+
+template <class C, typename R, int PASS, class Sink>
 __device__ __forceinline__ void jk_thread_passes(const JKSeg& sg, const JKQuartet& q, const double* __restrict__ tab,
                                                  const double* ri, const double* rj, const double* rk,
-                                                 const double* rl) {
+                                                 const double* rl, const Sink& sink) {
     constexpr int CI0 = PASS * C::GI;
     if constexpr (CI0 < C::NFI) {
         constexpr int CI1 = CI0 + C::GI < C::NFI ? CI0 + C::GI : C::NFI;
-        jk_thread_pass<C, R, CI0, CI1>(sg, q, tab, ri, rj, rk, rl);
-        jk_thread_passes<C, R, PASS + 1>(sg, q, tab, ri, rj, rk, rl);
+        jk_thread_pass<C, R, CI0, CI1>(sg, q, tab, ri, rj, rk, rl, sink);
+        jk_thread_passes<C, R, PASS + 1>(sg, q, tab, ri, rj, rk, rl, sink);
     }
 }
 
-template <class C, typename R>
-__device__ __forceinline__ void jk_thread_quartet(const JKSeg& sg, const JKQuartet& q, const double* __restrict__ tab) {
+template <class C, typename R, class Sink>
+__device__ __forceinline__ void jk_thread_quartet(const JKSeg& sg, const JKQuartet& q, const double* __restrict__ tab,
+                                                  const Sink& sink) {
     double ri[3], rj[3], rk[3], rl[3];
     load_center(sg, q.ish, ri);
     load_center(sg, q.jsh, rj);
     load_center(sg, q.ksh, rk);
     load_center(sg, q.lsh, rl);
-    jk_thread_passes<C, R, 0>(sg, q, tab, ri, rj, rk, rl);
+    jk_thread_passes<C, R, 0>(sg, q, tab, ri, rj, rk, rl, sink);
 }
 
 template <class C, typename R, class Src>
 __device__ __forceinline__ void jk_thread_body(const Src& src, double* jk_tab) {
-    rys_table_to_smem<C::NROOTS>(src.first().rys, jk_tab);
+    if constexpr (JKF32Prim<C, R>::value)
+        rys_table_to_smem_f<C::NROOTS>(src.first().rys, reinterpret_cast<float*>(jk_tab));
+    else
+        rys_table_to_smem<C::NROOTS>(src.first().rys, jk_tab);
     __syncthreads();
     // each warp takes a contiguous chunk of tasks (a multiple of 32); lane i
     // does tasks i, i+32, ... of it, so a warp covers consecutive kl of a row
@@ -379,7 +509,7 @@ __device__ __forceinline__ void jk_thread_body(const Src& src, double* jk_tab) {
         int row, col;
         const JKSeg& sg = cur.seek(src, t, row, col);
         JKQuartet q = jk_quartet_at(sg, row, col);
-        jk_thread_quartet<C, R>(sg, q, jk_tab);
+        jk_thread_quartet<C, R>(sg, q, jk_tab, jk_sink_global(sg));
     }
 }
 

@@ -254,6 +254,68 @@ def get_jk(mol, dm, hermi=1, vhfopt=None, with_j=True, with_k=True,
     return res[0], res[1]
 
 
+def get_jk_class_pairs(mol, dm, vhfopt, with_j=True, with_k=True,
+                       prescreen=True, nbins=None):
+    """J/K through the reference's own task loop (cuobc/scf/hf.py:104-166):
+    per-group absmax condensation of the densities, the class-level density
+    screen, log-Schwarz bins per class pair (``_make_s_index_offsets``) and
+    one ``jk_build_class_pair`` call per class quartet -- the GINTbuild_jk
+    contract (cuobc/lib/gvhf/nr_jk_driver.cu:227-284) on the per-class-pair
+    kernels.  Same result as :func:`get_jk` (which screens on the device and
+    runs the tiled kernels) up to rounding; returns CUDA tensors."""
+    torch = _torch()
+    lib = _lib.load_library()
+    nao, nao0 = vhfopt.coeff.shape
+    C = vhfopt.coeff_dev
+    d = torch.as_tensor(dm, dtype=torch.float64, device='cuda')
+    shape = tuple(d.shape)
+    d = d.reshape(-1, nao0, nao0)
+    n_dm = d.shape[0]
+    dms = (C @ d @ C.T).contiguous()
+    vj = torch.zeros(n_dm, nao, nao, dtype=torch.float64, device='cuda')
+    vk = torch.zeros_like(vj)
+    gao = vhfopt.mol.ao_loc_nr(cart=True)[vhfopt.l_ctr_offsets]
+    ng = len(gao) - 1
+    a = dms.abs().amax(0)
+    dm_cond = np.zeros((ng, ng))
+    for gi in range(ng):
+        rows = a[gao[gi]:gao[gi + 1]]
+        for gj in range(ng):
+            dm_cond[gi, gj] = float(rows[:, gao[gj]:gao[gj + 1]].max())
+    tol = vhfopt.direct_scf_tol
+    nbins = nbins if nbins is not None else vhfopt.default_nbins()
+    log_qs = vhfopt.log_qs
+    cp_idx, cp_jdx = np.tril_indices(ng)
+    sp = _stream_ptr(torch)
+    for cp_ij in range(len(log_qs)):
+        for cp_kl in range(cp_ij + 1):
+            lq_ij, lq_kl = log_qs[cp_ij], log_qs[cp_kl]
+            if lq_ij.size == 0 or lq_kl.size == 0:
+                continue
+            i, j, k, l = cp_idx[cp_ij], cp_jdx[cp_ij], cp_idx[cp_kl], cp_jdx[cp_kl]
+            sub = max(dm_cond[i, j], dm_cond[k, l], dm_cond[i, k],
+                      dm_cond[j, k], dm_cond[i, l], dm_cond[j, l])
+            if prescreen and sub < tol:
+                continue
+            with np.errstate(divide='ignore'):
+                cutoff = tol / sub
+            bij = _make_s_index_offsets(lq_ij, nbins, cutoff)
+            bkl = _make_s_index_offsets(lq_kl, nbins, cutoff)
+            _lib.check(lib.jk_build_class_pair(
+                vhfopt.handle, vj.data_ptr() if with_j else None,
+                vk.data_ptr() if with_k else None, dms.data_ptr(), nao, n_dm,
+                bij.ctypes.data, bkl.ctypes.data, nbins, cp_ij, cp_kl, sp),
+                'jk_build_class_pair')
+    out = []
+    for v, fac, on in ((vj, 2., with_j), (vk, 1., with_k)):
+        if not on:
+            out.append(None)
+            continue
+        w = fac * (C.T @ (v + v.transpose(1, 2)) @ C)
+        out.append(w.reshape(shape))
+    return out[0], out[1]
+
+
 def _get_jk(mf, mol=None, dm=None, hermi=1, with_j=True, with_k=True,
             omega=None):
     """RHF.get_jk of the reference (cuobc/scf/hf.py:230-250): builds and

@@ -108,6 +108,35 @@ def test_device_rys_tables_match_host():
                 np.testing.assert_allclose(w[i], hw, rtol=1e-14, atol=1e-300)
 
 
+def test_device_rys_fp32_nodes():
+    """Single-precision nodes and weights of the FP32 quartets (n <= 3):
+    nodes s = t^2 in [0, 1) within 2e-6 absolute, weights within 2e-6 of
+    their sum F0(x), against the double host evaluation."""
+    import torch
+    from byteqc_b200.cuobc import lib as jklib
+    lib = jklib.load_library()
+    rng = np.random.default_rng(2)
+    xs = np.concatenate([[0., 1e-9, 0.5, 0.7499, 0.75, 1.0, 2.0, 41.9, 42.0,
+                          47.99, 48.0, 53.99, 54.0, 200., 1e5],
+                         rng.uniform(0, 60, 300)])
+    dx = torch.as_tensor(xs, device='cuda')
+    for n in range(1, 4):
+        ds = torch.zeros(len(xs) * n, dtype=torch.float64, device='cuda')
+        dw = torch.zeros_like(ds)
+        assert lib.jk_rys_roots_device(n, dx.data_ptr(), len(xs), ds.data_ptr(),
+                                       dw.data_ptr(), 3, None) == 0
+        s = ds.cpu().numpy().reshape(-1, n)
+        w = dw.cpu().numpy().reshape(-1, n)
+        for i, x in enumerate(xs):
+            hs, hw = np.zeros(n), np.zeros(n)
+            lib.jk_rys_roots_host(n, x, hs.ctypes.data, hw.ctypes.data)
+            assert abs(s[i] - hs).max() <= 2e-6, (n, x, s[i], hs)
+            assert abs(w[i] - hw).max() <= 2e-6 * hw.sum(), (n, x, w[i], hw)
+    # higher orders are not evaluated in single precision
+    assert lib.jk_rys_roots_device(4, dx.data_ptr(), 1, ds.data_ptr(),
+                                   dw.data_ptr(), 3, None) != 0
+
+
 def test_mixed_precision_error_bounded():
     """FP32 recursion below the cutoff: J/K stay within a bound that scales
     with the cutoff, and fp32_cutoff=0 reproduces the FP64 engine exactly."""
@@ -124,3 +153,49 @@ def test_mixed_precision_error_bounded():
         mj, mk = hf.get_jk(mol, dm, vhfopt=opt, fp32_cutoff=cut)
         err = max(abs(mj - vj).max(), abs(mk - vk).max())
         assert err < 100 * cut, (cut, err)
+
+
+@pytest.mark.parametrize('case', ['h2o12-dz', 'walk30-631gs', 'h2o6-tzvp'])
+def test_tiled_matches_class_pair_loop(case):
+    """The device-screened tiled path (shared-memory digestion of chunk-pair
+    tiles) against the reference's task loop over jk_build_class_pair (host
+    bins, per-class-pair kernels): the same screened quartets, so the same
+    J/K within the FP64 bar, at sizes where most tiles digest in shared
+    memory; also J only, K only and two densities (global digestion)."""
+    from byteqc_b200.cuobc.scf import hf
+    if case == 'h2o12-dz':
+        mol = _mol(12, 'standin-cc-pvdz', 9.0, seed=5)
+    elif case == 'h2o6-tzvp':
+        mol = _mol(6, 'standin-def2-tzvp', 7.5, seed=6)
+    else:
+        mol = Mole(atom=geom.random_walk_molecule(30, seed=7),
+                   basis='standin-6-31g*').build()
+    s = mol.intor('int1e_ovlp')
+    dm = geom.scf_like_density(s, nocc=mol.nelectron // 2, seed=2)
+    opt = hf._VHFOpt(mol).build()
+    vj, vk = hf.get_jk(mol, dm, vhfopt=opt, out='device')
+    rj, rk = hf.get_jk_class_pairs(mol, dm, opt)
+    _close(vj.cpu().numpy(), rj.cpu().numpy())
+    _close(vk.cpu().numpy(), rk.cpu().numpy())
+    j1, k1 = hf.get_jk(mol, dm, vhfopt=opt, with_k=False, out='device')
+    assert k1 is None
+    _close(j1.cpu().numpy(), rj.cpu().numpy())
+    j2, k2 = hf.get_jk(mol, dm, vhfopt=opt, with_j=False, out='device')
+    assert j2 is None
+    _close(k2.cpu().numpy(), rk.cpu().numpy())
+    dm2 = np.stack([dm, 0.5 * dm])
+    vj2, vk2 = hf.get_jk(mol, dm2, vhfopt=opt, out='device')
+    _close(vj2[1].cpu().numpy(), 0.5 * rj.cpu().numpy())
+    _close(vk2[1].cpu().numpy(), 0.5 * rk.cpu().numpy())
+
+
+def test_tiled_vs_oracle_larger():
+    """A cluster large enough for shared-memory tiles, against the oracle."""
+    from byteqc_b200.cuobc.scf import hf
+    from oracle import hf_oracle
+    mol = _mol(5, 'standin-cc-pvdz', 6.5, seed=8)
+    dm = _rand_dm(mol.nao, seed=9)
+    vj, vk = hf.get_jk(mol, dm)
+    rj, rk = hf_oracle.get_jk(mol, dm)
+    _close(vj, rj)
+    _close(vk, rk)
