@@ -436,6 +436,17 @@ struct JKSeg {
     const double* dm;
     double* vj;
     double* vk;
+    // Pair-packed J side (jk_build): the density blocks of the pairs of the
+    // two classes, component-major (element c of pair p of a class at
+    // c * np + p), and accumulators of the same layout for the J
+    // contributions, added to vj after the launches.  Null: the kernels
+    // gather D and add J straight into vj.
+    const double* dp_ij;
+    const double* dp_kl;
+    double* jp_ij;
+    double* jp_kl;
+    int np_ij, np_kl;        // pairs of each class (component stride)
+    long long pk_stride;     // packed elements per density
 };
 
 // launchers of one class: a single segment (by value) or a segment table

@@ -323,6 +323,36 @@ __global__ void jk_screen_kernel(const JKScreenCQ* __restrict__ cqs, double tol,
     }
 }
 
+// Pair-packed J side of jk_build.  mode 0: gather the density blocks of
+// every pair into dp (element c of pair p of class k at off_k + c*np_k + p,
+// one copy per density); mode 1: add the packed J accumulators jp into vj.
+// Every (pair, component) is a distinct element of D and of vj.
+__global__ void jk_pack_kernel(const JKPackCls* __restrict__ cls, int ncls, long long total,
+                               const int* __restrict__ pair2bra, const int* __restrict__ pair2ket,
+                               const int* __restrict__ ao_loc, const double* __restrict__ dm, int nao, int n_dm,
+                               double* __restrict__ dp, const double* __restrict__ jp, double* __restrict__ vj,
+                               int mode) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = ncls - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (cls[mid].off <= t) lo = mid; else hi = mid - 1;
+        }
+        const JKPackCls k = cls[lo];
+        const long long local = t - k.off;
+        const int comp = (int)(local / k.np), p = (int)(local - (long long)comp * k.np);
+        const int a = comp / k.nfj, bb = comp - a * k.nfj;
+        const int pair = k.pair0 + p;
+        const size_t e = (size_t)(ao_loc[pair2bra[pair]] + a) + (size_t)nao * (ao_loc[pair2ket[pair]] + bb);
+        for (int m = 0; m < n_dm; m++) {
+            const size_t mo = (size_t)m * nao * nao;
+            if (mode == 0) dp[m * total + t] = dm[mo + e];
+            else vj[mo + e] += jp[m * total + t];
+        }
+    }
+}
+
 // J = 2 (V + V^T), K = V + V^T in place on the working-basis buffers, where
 // V[i, j] = mem[i + nao j]; out_rm[p, q] = fac (mem[p nao + q] + mem[q nao + p])
 __global__ void jk_symmetrize_kernel(const double* __restrict__ in, double* __restrict__ out, int nao, int n_dm,
@@ -366,6 +396,8 @@ static void free_basis(jk_basis* b) {
     cudaFree(b->d_qoff1);
     cudaFree(b->d_task01);
     cudaFree(b->d_work);
+    cudaFree(b->d_pack);
+    cudaFree(b->d_pk);
     if (b->h_qoff1) cudaFreeHost(b->h_qoff1);
     if (b->blas) cublasDestroy(b->blas);
     delete b;
@@ -624,6 +656,21 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
     }
     CUDA_TRY(upload(&b->d_cq, b->h_cq.data(), b->h_cq.size()));
     CUDA_TRY(cudaMalloc(&b->d_task01, sizeof(long long) * 2));
+    // pair-packed layout of the J side (jk_build)
+    b->h_pack.clear();
+    b->pack_total = 0;
+    for (int c = 0; c < b->ncp; c++) {
+        JKPackCls k;
+        k.off = b->pack_total;
+        k.pair0 = b->h_pair_locs[c];
+        k.np = b->h_pair_locs[c + 1] - k.pair0;
+        const int li = b->h_group_l[b->h_cls_gi[c]], lj = b->h_group_l[b->h_cls_gj[c]];
+        k.nfi = (li + 1) * (li + 2) / 2;
+        k.nfj = (lj + 1) * (lj + 2) / 2;
+        b->pack_total += (long long)k.np * k.nfi * k.nfj;
+        b->h_pack.push_back(k);
+    }
+    CUDA_TRY(upload(&b->d_pack, b->h_pack.data(), b->h_pack.size()));
     return JK_OK;
 }
 
@@ -704,6 +751,10 @@ static void fill_seg(const jk_basis* b, int cp_ij, int cp_kl, const long long* q
     s->dm = dm;
     s->vj = vj;
     s->vk = vk;
+    s->dp_ij = s->dp_kl = nullptr;
+    s->jp_ij = s->jp_kl = nullptr;
+    s->np_ij = s->np_kl = 0;
+    s->pk_stride = 0;
 }
 
 int jk_internal_class_index(const jk_basis_t* b, int cp_ij, int cp_kl);
@@ -728,10 +779,39 @@ extern "C" int jk_build(jk_basis_t* b, const double* dm, int n_dm, double* vj, d
     double fp32_cutoff = opts ? opts->fp32_cutoff : 0.;
     jk_screen_kernel<<<b->ncq, 256, 0, st>>>(b->d_cq, tol, nbins, prescreen, fp32_cutoff);
     CUDA_TRY(cudaGetLastError());
+    // pair-packed density and J accumulators for the thread kernels
+    const bool packed = vj && b->pack_total > 0;
+    double *dp = nullptr, *jp = nullptr;
+    const int pk_blocks = (int)std::min<long long>((b->pack_total + 255) / 256, (long long)b->nsm * 8);
+    if (packed) {
+        const size_t need = (size_t)2 * n_dm * b->pack_total;
+        if (need > b->pk_cap) {
+            cudaFree(b->d_pk);
+            b->d_pk = nullptr;
+            CUDA_TRY(cudaMalloc(&b->d_pk, sizeof(double) * need));
+            b->pk_cap = need;
+        }
+        dp = b->d_pk;
+        jp = b->d_pk + (size_t)n_dm * b->pack_total;
+        jk_pack_kernel<<<pk_blocks, 256, 0, st>>>(b->d_pack, b->ncp, b->pack_total, b->d_pair2bra, b->d_pair2ket,
+                                                   b->d_ao_loc, dm, b->nao, n_dm, dp, nullptr, nullptr, 0);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaMemsetAsync(jp, 0, sizeof(double) * n_dm * b->pack_total, st));
+    }
     for (int c = 0; c < b->ncq; c++) {
         const JKScreenCQ& cq = b->h_cq[c];
         JKSeg seg;
         fill_seg(b, cq.cp_ij, cq.cp_kl, b->d_qoff + cq.qoff_off, cq.n_ij, dm, n_dm, vj, vk, &seg);
+        if (packed) {
+            const JKPackCls &ki = b->h_pack[cq.cp_ij], &kk = b->h_pack[cq.cp_kl];
+            seg.dp_ij = dp + ki.off;
+            seg.dp_kl = dp + kk.off;
+            seg.jp_ij = jp + ki.off;
+            seg.jp_kl = jp + kk.off;
+            seg.np_ij = ki.np;
+            seg.np_kl = kk.np;
+            seg.pk_stride = b->pack_total;
+        }
         long long maxt = cq.cp_ij == cq.cp_kl ? (long long)cq.n_ij * (cq.n_ij + 1) / 2
                                               : (long long)cq.n_ij * cq.n_kl;
         int ci = class_index(b, cq.cp_ij, cq.cp_kl);
@@ -745,6 +825,11 @@ extern "C" int jk_build(jk_basis_t* b, const double* dm, int n_dm, double* vj, d
             seg.kl_base = b->d_klb + cq.qoff_off;
             CUDA_TRY(f32(seg, b->d_task032 + 2 * c, maxt, b->nsm, st));
         }
+    }
+    if (packed) {
+        jk_pack_kernel<<<pk_blocks, 256, 0, st>>>(b->d_pack, b->ncp, b->pack_total, b->d_pair2bra, b->d_pair2ket,
+                                                   b->d_ao_loc, dm, b->nao, n_dm, nullptr, jp, vj, 1);
+        CUDA_TRY(cudaGetLastError());
     }
     return JK_OK;
 }

@@ -37,6 +37,13 @@ void jk_internal_fill_seg(const jk_basis_t* b, int cp_ij, int cp_kl, const long 
 int jk_internal_launch(const jk_basis_t* b, int cp_ij, int cp_kl, const JKSeg& seg, const long long* d_task0,
                        long long max_tasks, void* stream);
 
+// one class pair in the pair-packed density / J buffers of jk_build
+struct JKPackCls {
+    long long off;      // first packed element of the class
+    int np, nfi, nfj;   // pairs, Cartesian components of the two shells
+    int pair0;          // first pair of the class
+};
+
 // Per-geometry state (opaque to callers of the C-ABI)
 struct jk_basis {
     // class quartets and their screening records
@@ -68,6 +75,12 @@ struct jk_basis {
     long long qoff1_cap = 0;
     long long* h_qoff1 = nullptr;  // pinned
     size_t h_qoff1_cap = 0;
+    // pair-packed J side of jk_build
+    std::vector<JKPackCls> h_pack;
+    JKPackCls* d_pack = nullptr;
+    long long pack_total = 0;  // packed elements per density
+    double* d_pk = nullptr;    // n_dm x pack_total densities, then as many J accumulators
+    size_t pk_cap = 0;
     // transform workspace
     cublasHandle_t blas = nullptr;
     double* d_work = nullptr;

@@ -45,6 +45,7 @@ __device__ __forceinline__ int jk_find_row(const long long* __restrict__ qoff, i
 struct JKQuartet {
     int ish, jsh, ksh, lsh;
     int prim_ij, prim_kl;  // first primitive pair of ij and kl
+    int row, col;          // pair indices within the two classes
     double norm;
 };
 
@@ -58,6 +59,8 @@ __device__ __forceinline__ JKQuartet jk_quartet_at(const JKSeg& sg, int row, int
     q.lsh = __ldg(sg.pair2ket + bkl);
     q.prim_ij = sg.prim_ij0 + row * sg.nprim_ij;
     q.prim_kl = sg.prim_kl0 + col * sg.nprim_kl;
+    q.row = row;
+    q.col = col;
     // 2 pi^3 / sqrt(pi), halved on the ij == kl diagonal (g2e.c:41, g2e.cu:1025)
     q.norm = JK_FAC * (bij == bkl ? 0.5 : 1.0);
     return q;
@@ -307,7 +310,44 @@ __device__ __forceinline__ void jk_thread_digest(const JKSeg& sg, const JKQuarte
 #define ACC(i, j, k, l) ((double)acc[(((i) * C::NFJ + (j)) * C::NFK + (k)) * C::NFL + (l)])
     for (int idm = 0; idm < sg.n_dm; idm++) {
         const double* D = sg.dm + (size_t)idm * nao * nao;
-        if (sg.vj) {
+        if (sg.vj && sg.dp_ij) {
+            // pair-packed: consecutive lanes hold consecutive kl pairs, so the
+            // D_kl loads and the J_kl additions are coalesced
+            const size_t po = (size_t)idm * sg.pk_stride;
+            const double* Dij = sg.dp_ij + po + q.row;
+            const double* Dkl = sg.dp_kl + po + q.col;
+#pragma unroll
+            for (int i = 0; i < NI; i++)
+#pragma unroll
+                for (int j = 0; j < C::NFJ; j++) {
+                    double v = 0;
+#pragma unroll
+                    for (int k = 0; k < C::NFK; k++)
+#pragma unroll
+                        for (int l = 0; l < C::NFL; l++)
+                            v += ACC(i, j, k, l) * __ldg(Dkl + (size_t)(k * C::NFL + l) * sg.np_kl);
+                    double* J = sg.jp_ij + po + (size_t)((CI0 + i) * C::NFJ + j) * sg.np_ij + q.row;
+                    if (wsame) {
+#pragma unroll
+                        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                        if ((threadIdx.x & 31) == 0) atomicAdd(J, v);
+                    } else {
+                        atomicAdd(J, v);
+                    }
+                }
+#pragma unroll
+            for (int k = 0; k < C::NFK; k++)
+#pragma unroll
+                for (int l = 0; l < C::NFL; l++) {
+                    double v = 0;
+#pragma unroll
+                    for (int i = 0; i < NI; i++)
+#pragma unroll
+                        for (int j = 0; j < C::NFJ; j++)
+                            v += ACC(i, j, k, l) * __ldg(Dij + (size_t)((CI0 + i) * C::NFJ + j) * sg.np_ij);
+                    atomicAdd(sg.jp_kl + po + (size_t)(k * C::NFL + l) * sg.np_kl + q.col, v);
+                }
+        } else if (sg.vj) {
 #pragma unroll
             for (int i = 0; i < NI; i++)
 #pragma unroll
