@@ -65,9 +65,10 @@ def batch_workload(nmol=256, seed=4, basis='standin-6-31g*'):
 
 
 def bench_batch(args, torch, timed):
-    """Batched builds of the 256-molecule workload: per-molecule launches,
-    one batched pass, the batch in mixed precision, and both from a captured
-    CUDA graph.  Returns the 'batch' sub-object of the bench line."""
+    """Builds of the 256-molecule workload: per-molecule launches in FP64 (the
+    plain engine), and the batch (one launch per shared class) replayed from a
+    captured CUDA graph in FP64 and in mixed precision.  Returns the 'batch'
+    sub-object of the bench line."""
     from byteqc_b200.cuobc.scf import hf
     from byteqc_b200.cuobc.scf.batch import JKBatch
     mols, dms = batch_workload(args.batch_mols)
@@ -82,10 +83,6 @@ def bench_batch(args, torch, timed):
         for m, d, o in zip(mols, d_dms, batch.opts):
             hf.get_jk(m, d, vhfopt=o, out='device')
 
-    def batched(cut):
-        def f():
-            batch._run(1, True, True, batch._opts(True, None, cut))
-        return f
     ref = batch.get_jk(d_dms, out='device')
 
     def err_vs_ref():
@@ -96,25 +93,19 @@ def bench_batch(args, torch, timed):
                    for a, b in zip(ref, got))
     batch._load(d_dms)
     res = {}
-    for name, fn in (('per_molecule_fp64', per_molecule),
-                     ('batched_fp64', batched(0.)),
-                     ('batched_mixed', batched(args.fp32_cutoff))):
-        for _ in range(2):
-            fn()
-        ms = timed(fn, max(2, args.steps))
-        res[name] = {'ms': ms, 'builds_per_s': len(mols) * 1e3 / ms}
-        if name.startswith('batched'):
-            res[name]['max_abs_err_jk_vs_fp64'] = err_vs_ref()
-    # graph replays
+    per_molecule()
+    ms = timed(per_molecule, args.batch_steps)
+    res['per_molecule_fp64'] = {'ms': ms, 'builds_per_s': len(mols) * 1e3 / ms}
     for name, cut in (('graph_fp64', 0.), ('graph_mixed', args.fp32_cutoff)):
         batch.capture(d_dms, fp32_cutoff=cut)
         g = batch._graph[0]
-        for _ in range(2):
-            g.replay()
-        ms = timed(g.replay, max(2, args.steps))
-        res[name] = {'ms': ms, 'builds_per_s': len(mols) * 1e3 / ms}
-        res[name]['max_abs_err_jk_vs_fp64'] = err_vs_ref()
+        g.replay()
+        ms = timed(g.replay, args.batch_steps)
+        res[name] = {'ms': ms, 'builds_per_s': len(mols) * 1e3 / ms,
+                     'max_abs_err_jk_vs_fp64': err_vs_ref()}
+    res['graph_mixed']['fp32_cutoff'] = args.fp32_cutoff
     base = res['per_molecule_fp64']['builds_per_s']
+    batch.close()
     return {'molecules': len(mols), 'basis': 'standin-6-31g*',
             'nbf_min': min(nbf), 'nbf_max': max(nbf), 'nbf_mean': float(np.mean(nbf)),
             'setup_s': setup, 'variants': res,
@@ -122,6 +113,97 @@ def bench_batch(args, torch, timed):
                 res['graph_mixed']['builds_per_s'] / base,
             'speedup_graph_mixed_vs_graph_fp64':
                 res['graph_mixed']['builds_per_s'] / res['graph_fp64']['builds_per_s']}
+
+
+def bench_sweep(args, torch, timed):
+    """Mixed-precision sweep on the (H2O)64 / cc-pVDZ workload: for each
+    fp32_cutoff the build time, the J/K max-abs error against the FP64
+    engine on the workload density, and the converged RHF energy against the
+    FP64 RHF energy."""
+    from byteqc_b200.cuobc.scf import RHF, hf
+    mol, dm = make_workload('h2o64-dz')
+    opt = hf._VHFOpt(mol).build()
+    d = torch.as_tensor(dm, device='cuda')
+    rj, rk = hf.get_jk(mol, d, vhfopt=opt, out='device')
+    ms64 = timed(lambda: hf.get_jk(mol, d, vhfopt=opt, out='device'), args.steps)
+    t = time.perf_counter()
+    mf = RHF(mol)
+    mf._opt_gpu = opt
+    e64 = mf.kernel()
+    scf64 = {'e_tot': e64, 'converged': mf.converged, 'cycles': mf.cycles,
+             'jk_builds': mf.jk_builds, 'wall_s': time.perf_counter() - t}
+    rows = []
+    for cut in args.sweep_cutoffs:
+        mj, mk = hf.get_jk(mol, d, vhfopt=opt, out='device', fp32_cutoff=cut)
+        err = max((mj - rj).abs().max().item(), (mk - rk).abs().max().item())
+        ms = timed(lambda: hf.get_jk(mol, d, vhfopt=opt, out='device',
+                                     fp32_cutoff=cut), args.steps)
+        t = time.perf_counter()
+        mf = RHF(mol, fp32_cutoff=cut)
+        mf._opt_gpu = opt
+        e = mf.kernel()
+        rows.append({'fp32_cutoff': cut, 'ms_per_build': ms,
+                     'speedup_vs_fp64': ms64 / ms, 'max_abs_err_jk': err,
+                     'scf_de': e - e64, 'converged': mf.converged,
+                     'cycles': mf.cycles, 'scf_wall_s': time.perf_counter() - t})
+    opt.clear()
+    return {'workload': 'h2o64-dz', 'nao': int(mol.nao), 'ms_per_build_fp64': ms64,
+            'scf_fp64': scf64, 'rows': rows}
+
+
+def serve_workload(nreq, seed=5, max_nbf=2000, min_nbf=50):
+    """Requests of the serving stream: seeded random-walk molecules sized
+    log-uniform in [min_nbf, max_nbf] basis functions, the basis drawn from
+    6-31G*, cc-pVDZ and def2-TZVP (stand-ins)."""
+    from byteqc_b200.gto import Mole, geom
+    rng = np.random.default_rng(seed)
+    per_atom = {'standin-6-31g*': 8.5, 'standin-cc-pvdz': 9.5,
+                'standin-def2-tzvp': 18.5}
+    bases = sorted(per_atom)
+    mols = []
+    for i in range(nreq):
+        basis = bases[int(rng.integers(len(bases)))]
+        nbf = float(np.exp(rng.uniform(np.log(min_nbf), np.log(max_nbf))))
+        natm = max(3, int(round(nbf / per_atom[basis])))
+        mols.append(Mole(atom=geom.random_walk_molecule(natm, seed=seed * 7919 + i),
+                         basis=basis).build())
+    return mols
+
+
+def bench_serve(args, torch):
+    """Continuous-batching server on a Poisson stream: the closed-loop
+    capacity (all requests queued at once), then arrivals at 80 % of that
+    rate in FP64 and in mixed precision; per-build p50/p99 latency and
+    builds/s."""
+    from byteqc_b200.cuobc.scf.serve import JKServer, poisson_serve
+    mols = serve_workload(args.serve_requests, max_nbf=args.serve_max_nbf)
+    nbf = [m.nao for m in mols]
+    kw = dict(n_iter=args.serve_iters)
+    # warm-up: kernels, attributes, allocator
+    warm = JKServer(**kw)
+    for m in mols[:2]:
+        warm.submit(m)
+    warm.run_until_empty()
+    t = time.perf_counter()
+    srv = JKServer(**kw)
+    for m in mols:
+        srv.submit(m)
+    srv.run_until_empty()
+    wall = time.perf_counter() - t
+    cap_builds = srv.builds / wall
+    rate = 0.8 * cap_builds / args.serve_iters  # requests per second
+    out = {'requests': len(mols), 'iters_per_request': args.serve_iters,
+           'nbf_min': min(nbf), 'nbf_max': max(nbf), 'nbf_median': float(np.median(nbf)),
+           'closed_loop': dict(srv.stats(), builds_per_s=cap_builds, wall_s=wall),
+           'poisson_rate_req_per_s': rate}
+    for name, cut in (('fp64', None), ('mixed', args.fp32_cutoff)):
+        srv, wall = poisson_serve(mols, rate, seed=5, fp32_cutoff=cut, **kw)
+        st = srv.stats()
+        st.update(builds_per_s=srv.builds / wall, wall_s=wall)
+        if cut:
+            st['fp32_cutoff'] = cut
+        out[name] = st
+    return out
 
 
 def ncart(l):
@@ -199,40 +281,61 @@ class ClockSampler:
                 'reasons': sorted(reasons), 'samples': len(self.samples)}
 
 
-def cpu_baseline(mol, dm, target_s=15.0):
-    """Oracle J/K on all host cores over a uniform subsample of ij rows,
-    scaled to one full build.  Returns (builds/s, info)."""
+def cpu_baseline(mol, dm, target_s=15.0, opt=None, repeats=1):
+    """Oracle J/K on all host cores over a uniform subsample of ij rows
+    (rows ij = stride/2 mod stride of every class pair), scaled to one full
+    build by exact quartet counts: a count-only pass gives the quartets of
+    the full build and the build's fixed cost (density transforms, final
+    contraction), the sample its time per quartet.  Returns (builds/s, info)."""
     from oracle import hf_oracle
-    opt = hf_oracle.VHFOpt(mol).build()
-    t = time.perf_counter()
-    hf_oracle.get_jk(mol, dm, vhfopt=opt, ij_stride=4096)
-    t0 = time.perf_counter() - t
-    full = t0 * 4096
-    stride = 1
-    while full / stride > target_s and stride < 4096:
-        stride *= 2
+    if opt is None:
+        opt = hf_oracle.VHFOpt(mol).build()
     st = {}
+    hf_oracle.get_jk(mol, dm, vhfopt=opt, count_only=True, stats=st)  # warm-up
     t = time.perf_counter()
-    hf_oracle.get_jk(mol, dm, vhfopt=opt, ij_stride=stride, stats=st)
-    dt = time.perf_counter() - t
-    est = dt * stride
+    hf_oracle.get_jk(mol, dm, vhfopt=opt, count_only=True, stats=st)
+    fixed = time.perf_counter() - t
+    total = st['quartets']
+
+    def sample(stride):
+        s2 = {}
+        t = time.perf_counter()
+        hf_oracle.get_jk(mol, dm, vhfopt=opt, ij_stride=stride,
+                         ij_offset=stride // 2, stats=s2)
+        return time.perf_counter() - t, s2['quartets']
+    # calibration: quartets per second of a small sample, its fixed cost
+    # included (a lower bound of the rate, so the sample stays bounded)
+    stride = 256
+    dt, q = sample(stride)
+    rate = max(q, 1) / max(dt, 1e-3)
+    stride = int(min(1 << 20, max(1, round(total / max(rate * target_s, 1.0)))))
+    vals = []
+    for _ in range(repeats):
+        dt, q = sample(stride)
+        # per-quartet time from the sample beyond the fixed cost; when the
+        # sample is too small to separate them, its whole time per quartet
+        work = dt - fixed if dt > 2 * fixed else dt
+        est = (fixed if dt > 2 * fixed else 0.) + work * total / max(q, 1)
+        vals.append(1.0 / est)
     cores = int(os.environ.get('OMP_NUM_THREADS', os.cpu_count() or 1))
-    return 1.0 / est, {'cores': cores, 'stride': stride, 'sample_s': dt,
-                       'sample_quartets': st.get('quartets')}
+    info = {'cores': cores, 'stride': stride, 'sample_s': dt,
+            'sample_quartets': q, 'total_quartets': total,
+            'fixed_s': fixed, 'est_build_s': est}
+    return (vals if repeats > 1 else vals[0]), info
 
 
 def run_reference(args):
+    """The reference arm: the oracle (a port of the reference's CPU algorithm
+    for this path) on all host cores, rank 0 only; every step is one bounded
+    sample of the build, scaled by quartet count."""
     rank = int(os.environ.get('RANK', '0'))
     if rank != 0:
         return
     mol, dm = make_workload(args.workload)
-    vals = []
-    info = None
-    for i in range(args.warmup + args.steps):
-        v, info = cpu_baseline(mol, dm, target_s=args.ref_sample_s)
-        if i >= args.warmup:
-            vals.append(v)
-    value = float(np.median(vals))
+    vals, info = cpu_baseline(mol, dm, target_s=args.ref_sample_s,
+                              repeats=args.warmup + args.steps)
+    vals = vals if isinstance(vals, list) else [vals]
+    value = float(np.median(vals[args.warmup:] or vals))
     line = {
         'impl': 'reference', 'metric': 'jk_builds_per_s', 'value': value,
         'unit': 'builds/s', 'n_gpus': args.gpus, 'steps': args.steps,
@@ -242,9 +345,9 @@ def run_reference(args):
         'cpu_baseline': {
             'value': value, 'unit': 'builds/s', 'cores': info['cores'],
             'kind': 'port',
-            'sample': 'oracle J/K on every %d-th shell-pair row of each '
-                      'class pair (%.1f s of CPU work), scaled to one build'
-                      % (info['stride'], info['sample_s'])},
+            'sample': ('oracle J/K on every %d-th shell-pair row of each class pair (%d of %d quartets, %.1f s of CPU work), scaled to one build by quartet count'
+                       % (info['stride'], info['sample_quartets'],
+                          info['total_quartets'], info['sample_s']))},
         'e2e': {'value': value, 'unit': 'builds/s', 'h2d_bytes_per_step': 0,
                 'd2h_bytes_per_step': 0},
     }
@@ -259,9 +362,21 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--workload', default='h2o32-tzvp', choices=sorted(WORKLOADS))
     ap.add_argument('--no-cpu-baseline', action='store_true')
-    ap.add_argument('--ref-sample-s', type=float, default=12.0)
+    ap.add_argument('--ref-sample-s', type=float, default=8.0)
     ap.add_argument('--batch-mols', type=int, default=256,
                     help='molecules of the batched workload (0: skip)')
+    ap.add_argument('--batch-steps', type=int, default=1,
+                    help='timed repetitions of each batched variant')
+    ap.add_argument('--no-sweep', action='store_true',
+                    help='skip the mixed-precision cutoff sweep with SCF energies')
+    ap.add_argument('--sweep-cutoffs', type=float, nargs='*',
+                    default=[1e-8, 1e-7, 1e-6, 1e-5, 1e-4])
+    ap.add_argument('--serve-requests', type=int, default=16,
+                    help='requests of the serving stream (0: skip)')
+    ap.add_argument('--serve-iters', type=int, default=15)
+    ap.add_argument('--serve-max-nbf', type=int, default=600,
+                    help='largest request in basis functions (2000 for the '
+                         'full 50-2000 range)')
     ap.add_argument('--fp32-cutoff', type=float, default=1e-6,
                     help='also time the mixed-precision build at this cutoff '
                          '(0: skip)')
@@ -386,7 +501,11 @@ def main():
                              + fj * fl)
     peak = ctypes.c_double()
     lib.jk_fma_peak(0, ctypes.byref(peak))
+    peak32 = ctypes.c_double()
+    lib.jk_fma_peak(1, ctypes.byref(peak32))
     achieved = flops / (ms_kern * 1e-3) / 1e12
+    # the last build was the mixed one when it ran: its FP32 share of quartets
+    f32_share = float(counts2[ncq:2 * ncq].sum()) / max(1, quartets)
 
     if rank != 0:
         if dist:
@@ -425,22 +544,29 @@ def main():
                 'd2h_bytes_per_step': int(2 * dm.nbytes)},
         'clocks': clk.summary(),
     }
-    if args.batch_mols > 0:
+    if args.batch_mols > 0 and world == 1:
         line['batch'] = bench_batch(args, torch, timed)
+    if not args.no_sweep and world == 1:
+        line['sweep'] = bench_sweep(args, torch, timed)
+    if args.serve_requests > 0 and world == 1:
+        line['serve'] = bench_serve(args, torch)
     if ms_mixed is not None:
         line['mixed'] = {'fp32_cutoff': args.fp32_cutoff,
                          'value': world * 1e3 / ms_mixed, 'unit': 'builds/s',
                          'ms_per_step': ms_mixed,
                          'speedup_vs_fp64': ms_step / ms_mixed,
-                         'max_abs_err_jk': mixed_err}
+                         'max_abs_err_jk': mixed_err,
+                         'fp32_quartet_share': f32_share,
+                         'achieved_tflops': flops / (ms_mixed * 1e-3) / 1e12,
+                         'peak_fp32_tflops': peak32.value}
     if world == 1 and not args.no_cpu_baseline:
         v, inf = cpu_baseline(mol, dm)
         line['cpu_baseline'] = {
             'value': v, 'unit': 'builds/s', 'cores': inf['cores'],
             'kind': 'port',
-            'sample': 'oracle J/K on every %d-th shell-pair row of each class '
-                      'pair (%.1f s of CPU work), scaled to one build'
-                      % (inf['stride'], inf['sample_s'])}
+            'sample': ('oracle J/K on every %d-th shell-pair row of each class pair (%d of %d quartets, %.1f s of CPU work), scaled to one build by quartet count'
+                       % (inf['stride'], inf['sample_quartets'],
+                          inf['total_quartets'], inf['sample_s']))}
     print(json.dumps(line, default=float))
     if dist:
         dist.destroy_process_group()

@@ -300,12 +300,16 @@ __device__ __forceinline__ void jk_thread_digest(const JKSeg& sg, const JKQuarte
     const int i0 = __ldg(sg.ao_loc + q.ish) + CI0, j0 = __ldg(sg.ao_loc + q.jsh);
     const int k0 = __ldg(sg.ao_loc + q.ksh), l0 = __ldg(sg.ao_loc + q.lsh);
     // the lanes of a warp usually share the ij pair (consecutive kl of one
-    // row): then the J_ij block is summed over the warp before it is added
+    // row): then the J_ij block is summed over the warp before it is added.
+    // In a batched launch a warp can straddle two molecules whose shells
+    // carry the same indices, so the lanes must also share the output.
     const unsigned am = __activemask();
     bool wsame = false;
     if (am == 0xffffffffu) {
+        const unsigned long long out = (unsigned long long)(sg.jp_ij ? (const void*)sg.jp_ij : (const void*)sg.vj);
         int i_0 = __shfl_sync(am, q.ish, 0), j_0 = __shfl_sync(am, q.jsh, 0);
-        wsame = __all_sync(am, q.ish == i_0 && q.jsh == j_0);
+        unsigned long long o_0 = __shfl_sync(am, out, 0);
+        wsame = __all_sync(am, q.ish == i_0 && q.jsh == j_0 && out == o_0);
     }
 #define ACC(i, j, k, l) ((double)acc[(((i) * C::NFJ + (j)) * C::NFK + (k)) * C::NFL + (l)])
     for (int idm = 0; idm < sg.n_dm; idm++) {

@@ -204,9 +204,13 @@ def _ptr(a):
 
 
 def get_jk(mol, dm, hermi=1, vhfopt=None, with_j=True, with_k=True,
-           prescreen=True, nbins=None, stats=None, ij_stride=1):
+           prescreen=True, nbins=None, stats=None, ij_stride=1, ij_offset=0,
+           count_only=False):
     """Oracle J/K.  Returns numpy (vj, vk) shaped like ``dm``; a disabled
-    matrix is None."""
+    matrix is None.  ``ij_stride``/``ij_offset`` evaluate only the rows
+    ij = ij_offset mod ij_stride of every class pair (a subsample for timing);
+    ``count_only`` evaluates nothing and only counts the quartets (in
+    ``stats['quartets']``)."""
     if hermi != 1:
         raise NotImplementedError('JK-builder only supports hermitian '
                                   'density matrix')
@@ -237,6 +241,10 @@ def get_jk(mol, dm, hermi=1, vhfopt=None, with_j=True, with_k=True,
     ao_loc = pmol.ao_loc_nr(cart=True)
     lib = oracle.lib()
     nquartets = 0
+    if not count_only and lib.oracle_jk_begin(
+            ctypes.c_int(nao), ctypes.c_int(n_dm), ctypes.c_int(int(with_j)),
+            ctypes.c_int(int(with_k))):
+        raise MemoryError('oracle J/K accumulators')
     for n in range(ncptype * (ncptype + 1) // 2):
         cp_ij = int(np.floor(np.sqrt(2 * n)))
         if cp_ij * (cp_ij + 1) // 2 > n:
@@ -262,7 +270,11 @@ def get_jk(mol, dm, hermi=1, vhfopt=None, with_j=True, with_k=True,
             ctypes.c_int(nao), ctypes.c_int(n_dm),
             _ptr(vj) if with_j else None, _ptr(vk) if with_k else None,
             _ptr(bins_ij), _ptr(bins_kl), ctypes.c_int(nbins),
-            ctypes.c_int(cp_ij), ctypes.c_int(cp_kl), ctypes.c_int(ij_stride))
+            ctypes.c_int(cp_ij), ctypes.c_int(cp_kl), ctypes.c_int(ij_stride),
+            ctypes.c_int(ij_offset), ctypes.c_int(int(count_only)))
+    if not count_only:
+        lib.oracle_jk_end(_ptr(vj) if with_j else None,
+                          _ptr(vk) if with_k else None)
     if stats is not None:
         stats['quartets'] = nquartets
         stats['nbins'] = nbins

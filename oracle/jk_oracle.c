@@ -265,23 +265,53 @@ void oracle_q_cond(const int *atm, const int *bas, const double *env, int nbas, 
  * reference bin offsets (host arrays, nbins+1 entries, local to the class),
  * accumulated into vj/vk (either may be NULL) with the reference's view
  * convention v[i + nao*j].  pair_locs: start of each class in pair2bra/ket.
- * ij_stride > 1 evaluates only the rows ij = 0 mod ij_stride (a uniform
- * subsample used to time the CPU baseline on a bounded share of the work).
+ * ij_stride > 1 evaluates only the rows ij = ij_offset mod ij_stride (a
+ * uniform subsample used to time the CPU baseline on a bounded share of the
+ * work); count_only returns the number of quartets without evaluating them.
  * dm: (n_dm, nao, nao) C-order.  Returns the number of contracted quartets
  * evaluated.
+ *
+ * Between oracle_jk_begin and oracle_jk_end the per-thread accumulators live
+ * across calls (allocated and zeroed once, summed into vj/vk once by
+ * oracle_jk_end); otherwise every call allocates and reduces its own.
  */
+static double *g_vjt = NULL, *g_vkt = NULL;
+static size_t g_nn = 0;
+
+int oracle_jk_begin(int nao, int n_dm, int with_j, int with_k) {
+    g_nn = (size_t)nao * nao * n_dm;
+    int nthreads = omp_get_max_threads();
+    g_vjt = with_j ? calloc(g_nn * nthreads, sizeof(double)) : NULL;
+    g_vkt = with_k ? calloc(g_nn * nthreads, sizeof(double)) : NULL;
+    return ((with_j && !g_vjt) || (with_k && !g_vkt)) ? 1 : 0;
+}
+
+void oracle_jk_end(double *vj, double *vk) {
+    int nthreads = omp_get_max_threads();
+    for (int t = 0; t < nthreads; t++)
+        for (size_t x = 0; x < g_nn; x++) {
+            if (vj && g_vjt) vj[x] += g_vjt[g_nn * t + x];
+            if (vk && g_vkt) vk[x] += g_vkt[g_nn * t + x];
+        }
+    free(g_vjt);
+    free(g_vkt);
+    g_vjt = g_vkt = NULL;
+    g_nn = 0;
+}
+
 long oracle_build_jk(const int *atm, const int *bas, const double *env, int nbas, const int *ao_loc,
                      const int *pair2bra, const int *pair2ket, const int *pair_locs, double diag_fac,
                      const double *dm, int nao, int n_dm, double *vj, double *vk,
                      const int *bins_ij, const int *bins_kl, int nbins, int cp_ij, int cp_kl,
-                     int ij_stride) {
+                     int ij_stride, int ij_offset, int count_only) {
     basis_t b = {atm, bas, env, nbas};
     double fac = 2 * M_PI * M_PI * M_PI / sqrt(M_PI);
     long count = 0;
     size_t nn = (size_t)nao * nao * n_dm;
     int nthreads = omp_get_max_threads();
-    double *vjt = vj ? calloc(nn * nthreads, sizeof(double)) : NULL;
-    double *vkt = vk ? calloc(nn * nthreads, sizeof(double)) : NULL;
+    const int shared_ws = g_nn == nn && (g_vjt || g_vkt);
+    double *vjt = (vj && !count_only) ? (shared_ws ? g_vjt : calloc(nn * nthreads, sizeof(double))) : NULL;
+    double *vkt = (vk && !count_only) ? (shared_ws ? g_vkt : calloc(nn * nthreads, sizeof(double))) : NULL;
     for (int kl_bin = 0; kl_bin < nbins; kl_bin++) {
         int kl0 = bins_kl[kl_bin], kl1 = bins_kl[kl_bin + 1];
         if (kl1 - kl0 <= 0) continue;
@@ -291,16 +321,20 @@ long oracle_build_jk(const int *atm, const int *bas, const double *env, int nbas
 #pragma omp parallel reduction(+ : count)
         {
             int tid = omp_get_thread_num();
-            double *myj = vj ? vjt + nn * tid : NULL;
-            double *myk = vk ? vkt + nn * tid : NULL;
+            double *myj = vjt ? vjt + nn * tid : NULL;
+            double *myk = vkt ? vkt + nn * tid : NULL;
             double *g = malloc(sizeof(double) * NF_MAX * NF_MAX * NF_MAX * NF_MAX);
 #pragma omp for schedule(static)
-            for (int tij = ij0; tij < ij1; tij++)
+            for (int tij = ij0; tij < ij1; tij++) {
+                if (ij_stride > 1 && tij % ij_stride != ij_offset) continue;
                 for (int tkl = kl0; tkl < kl1; tkl++) {
-                    if (ij_stride > 1 && tij % ij_stride) continue;
                     int bas_ij = pair_locs[cp_ij] + tij;
                     int bas_kl = pair_locs[cp_kl] + tkl;
                     if (bas_ij < bas_kl) continue;
+                    if (count_only) {
+                        count++;
+                        continue;
+                    }
                     double norm = fac;
                     if (bas_ij == bas_kl) norm *= .5;
                     int ish = pair2bra[bas_ij], jsh = pair2ket[bas_ij];
@@ -333,15 +367,18 @@ long oracle_build_jk(const int *atm, const int *bas, const double *env, int nbas
                                     }
                     }
                 }
+            }
             free(g);
         }
     }
-    for (int t = 0; t < nthreads; t++)
-        for (size_t x = 0; x < nn; x++) {
-            if (vj) vj[x] += vjt[nn * t + x];
-            if (vk) vk[x] += vkt[nn * t + x];
-        }
-    free(vjt);
-    free(vkt);
+    if (!shared_ws) {
+        for (int t = 0; t < nthreads; t++)
+            for (size_t x = 0; x < nn; x++) {
+                if (vjt) vj[x] += vjt[nn * t + x];
+                if (vkt) vk[x] += vkt[nn * t + x];
+            }
+        free(vjt);
+        free(vkt);
+    }
     return count;
 }

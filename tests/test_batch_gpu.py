@@ -59,3 +59,22 @@ def test_batch_graph_replay():
     for (aj, ak), (bj, bk) in zip(ref1, got):
         assert abs(aj - bj).max() <= 1e-10 * max(1.0, abs(aj).max())
         assert abs(ak - bk).max() <= 1e-10 * max(1.0, abs(ak).max())
+
+
+def test_batch_identical_molecules_keep_their_own_j():
+    """Copies of one molecule in a batch: their segments of a class carry the
+    same shell indices, so a warp that straddles two of them must not merge
+    their J contributions (each copy has its own density)."""
+    from byteqc_b200.cuobc.scf import hf
+    from byteqc_b200.cuobc.scf.batch import JKBatch
+    atoms = geom.water_cluster(1, box=4.0, seed=3)
+    mols = [Mole(atom=atoms, basis='standin-cc-pvdz').build() for _ in range(6)]
+    dms = _dms(mols, seed=5)
+    batch = JKBatch(mols)
+    for cut in (None, 1e-6):
+        res = batch.get_jk(dms, fp32_cutoff=cut)
+        for m, (mol, dm, opt) in enumerate(zip(mols, dms, batch.opts)):
+            vj, vk = hf.get_jk(mol, dm, vhfopt=opt, fp32_cutoff=cut)
+            scale = max(1.0, abs(vj).max())
+            assert abs(res[m][0] - vj).max() <= 1e-10 * scale, (cut, m)
+            assert abs(res[m][1] - vk).max() <= 1e-10 * scale, (cut, m)
