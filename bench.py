@@ -303,12 +303,15 @@ def cpu_baseline(mol, dm, target_s=15.0, opt=None, repeats=1):
         hf_oracle.get_jk(mol, dm, vhfopt=opt, ij_stride=stride,
                          ij_offset=stride // 2, stats=s2)
         return time.perf_counter() - t, s2['quartets']
-    # calibration: quartets per second of a small sample, its fixed cost
-    # included (a lower bound of the rate, so the sample stays bounded)
-    stride = 256
-    dt, q = sample(stride)
-    rate = max(q, 1) / max(dt, 1e-3)
-    stride = int(min(1 << 20, max(1, round(total / max(rate * target_s, 1.0)))))
+    # calibration: quadruple the sample until its work beyond the fixed cost
+    # reaches a quarter of the target (the samples grow geometrically, so the
+    # calibration costs about a third of the final sample)
+    stride = 1 << 14
+    while True:
+        dt, q = sample(stride)
+        if stride == 1 or dt - fixed >= 0.25 * target_s:
+            break
+        stride = max(1, stride // 4)
     vals = []
     for _ in range(repeats):
         dt, q = sample(stride)

@@ -324,10 +324,16 @@ long oracle_build_jk(const int *atm, const int *bas, const double *env, int nbas
             double *myj = vjt ? vjt + nn * tid : NULL;
             double *myk = vkt ? vkt + nn * tid : NULL;
             double *g = malloc(sizeof(double) * NF_MAX * NF_MAX * NF_MAX * NF_MAX);
-#pragma omp for schedule(static)
-            for (int tij = ij0; tij < ij1; tij++) {
-                if (ij_stride > 1 && tij % ij_stride != ij_offset) continue;
+            // rows of the (sub)sample; the loop runs over (row, kl) so that a
+            // subsample with few rows still uses every thread
+            const int rstep = ij_stride > 1 ? ij_stride : 1;
+            int r0 = ij0;
+            if (rstep > 1) r0 = ij0 + ((ij_offset - ij0 % rstep) % rstep + rstep) % rstep;
+            const int nrows = r0 < ij1 ? (ij1 - 1 - r0) / rstep + 1 : 0;
+#pragma omp for collapse(2) schedule(dynamic, 64)
+            for (int ri = 0; ri < nrows; ri++) {
                 for (int tkl = kl0; tkl < kl1; tkl++) {
+                    const int tij = r0 + ri * rstep;
                     int bas_ij = pair_locs[cp_ij] + tij;
                     int bas_kl = pair_locs[cp_kl] + tkl;
                     if (bas_ij < bas_kl) continue;

@@ -156,12 +156,12 @@ def test_mixed_precision_error_bounded():
 
 
 @pytest.mark.parametrize('case', ['h2o12-dz', 'walk30-631gs', 'h2o6-tzvp'])
-def test_tiled_matches_class_pair_loop(case):
-    """The device-screened tiled path (shared-memory digestion of chunk-pair
-    tiles) against the reference's task loop over jk_build_class_pair (host
-    bins, per-class-pair kernels): the same screened quartets, so the same
-    J/K within the FP64 bar, at sizes where most tiles digest in shared
-    memory; also J only, K only and two densities (global digestion)."""
+def test_device_screen_matches_class_pair_loop(case):
+    """get_jk (screening on the device, pair-packed J side) against the
+    reference's task loop over jk_build_class_pair (host bins, direct
+    digestion): the same screened quartets, so the same J/K within the FP64
+    bar, at sizes well beyond the oracle's reach; also J only, K only and two
+    densities."""
     from byteqc_b200.cuobc.scf import hf
     if case == 'h2o12-dz':
         mol = _mol(12, 'standin-cc-pvdz', 9.0, seed=5)
@@ -189,8 +189,9 @@ def test_tiled_matches_class_pair_loop(case):
     _close(vk2[1].cpu().numpy(), 0.5 * rk.cpu().numpy())
 
 
-def test_tiled_vs_oracle_larger():
-    """A cluster large enough for shared-memory tiles, against the oracle."""
+def test_get_jk_vs_oracle_larger():
+    """A five-water cluster (long kl rows, many class quartets) against the
+    oracle."""
     from byteqc_b200.cuobc.scf import hf
     from oracle import hf_oracle
     mol = _mol(5, 'standin-cc-pvdz', 6.5, seed=8)
@@ -199,3 +200,16 @@ def test_tiled_vs_oracle_larger():
     rj, rk = hf_oracle.get_jk(mol, dm)
     _close(vj, rj)
     _close(vk, rk)
+
+
+@pytest.mark.parametrize('case', ['h2o-dz', 'h2o2-tzvp', 'walk6-631gs'])
+def test_get_jk_vs_golden(case):
+    """The engine against the committed golden J/K (tests/golden)."""
+    import os
+    from byteqc_b200.cuobc.scf import hf
+    from tests.golden.make_golden import case_inputs
+    g = np.load(os.path.join(os.path.dirname(__file__), 'golden', 'golden_jk.npz'))
+    mol, dm = case_inputs(case)
+    vj, vk = hf.get_jk(mol, dm)
+    _close(vj, g[case + '/vj'])
+    _close(vk, g[case + '/vk'])

@@ -1,0 +1,116 @@
+"""The oracle itself (CPU, no GPU): pinned against an independent integral
+algorithm (Obara-Saika / Head-Gordon-Pople on scipy's Boys function,
+oracle/eri_os.py), a closed form, a brute-force contraction of the full ERI
+tensor, and the committed golden J/K fixtures (tests/golden)."""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from byteqc_b200.gto import Mole, geom
+
+GOLDEN = os.path.join(os.path.dirname(__file__), 'golden', 'golden_jk.npz')
+
+
+def _pmol(nw, basis, box, seed):
+    from oracle import hf_oracle
+    mol = Mole(atom=geom.water_cluster(nw, box=box, seed=seed),
+               basis=basis).build()
+    return hf_oracle.VHFOpt(mol).build().mol
+
+
+def test_ss_closed_form():
+    """(s_A s_A | s_B s_B) of single s primitives: with p = q = 2a,
+    (c f)^4 2 pi^2.5 / (p q sqrt(p+q)) F0(T), T = a |AB|^2 and
+    F0(T) = sqrt(pi/T) erf(sqrt T) / 2 (c the stored coefficient, f the
+    libcint s-factor)."""
+    import oracle
+    from oracle import eri_os
+    mol = Mole(atom=[('H', (0., 0., 0.)), ('H', (0., 0., 0.9))],
+               basis={'H': [[0, [1.3, 1.0]]]}, cart=True).build()
+    a = 1.3
+    A, B = mol.atom_coords()
+    c = mol.bas_ctr_coeff(0)[0, 0]
+    p = q = 2 * a
+    T = p * q / (p + q) * float(np.dot(A - B, A - B))
+    f0 = math.sqrt(math.pi / T) * math.erf(math.sqrt(T)) / 2
+    ref = (c * eri_os.FAC_SP[0]) ** 4 * 2 * math.pi ** 2.5 / (p * q * math.sqrt(p + q)) * f0
+    got = oracle.eri_shells(mol, 0, 0, 1, 1)[0, 0, 0, 0]
+    assert abs(got - ref) <= 1e-14 * abs(ref)
+
+
+def test_rys_quadrature_exact_on_moments():
+    """sum_r w_r t_r^(2k) = F_k(x) for k < 2n (the Rys rule integrates the
+    Boys moments exactly), n = 1..11 on x in [0, 120]."""
+    import oracle
+    from oracle.eri_os import boys
+    for n in range(1, 12):
+        for x in (0.0, 0.3, 1.7, 6.0, 25.0, 60.0, 119.0):
+            s, w = oracle.rys_roots(n, x)
+            for k in range(2 * n):
+                lhs = float(np.sum(w * s ** k))
+                rhs = boys(k, x)
+                assert abs(lhs - rhs) <= 1e-12 * max(abs(rhs), 1e-30) + 1e-300, (n, x, k)
+
+
+def test_eri_vs_obara_saika():
+    """Contracted Cartesian shell quartets up to (ff|ff) from the oracle's Rys
+    engine against Obara-Saika."""
+    import oracle
+    from oracle import eri_os
+    pm = _pmol(1, 'standin-def2-tzvp', 4.0, 1)
+    rng = np.random.default_rng(0)
+    ls = pm._bas[:, 1]
+    by_l = {l: np.flatnonzero(ls == l) for l in range(4)}
+    picks = [(3, 3, 3, 3), (3, 2, 1, 0), (2, 2, 2, 1), (1, 1, 1, 1), (3, 0, 2, 0)]
+    for lq in picks:
+        sh = [int(rng.choice(by_l[l])) for l in lq]
+        a = oracle.eri_shells(pm, *sh)
+        b = eri_os.eri_shells(pm, *sh)
+        assert a.shape == b.shape
+        # relative to the block's largest element, with an absolute floor for
+        # blocks that vanish by symmetry (one-centre, odd total parity)
+        assert abs(a - b).max() <= 1e-12 * abs(b).max() + 1e-14, lq
+
+
+def test_jk_vs_full_eri_tensor():
+    """Oracle get_jk (screened, binned, 8-fold symmetric loop) against J and K
+    contracted from the full ERI tensor of the working basis."""
+    import oracle
+    from oracle import hf_oracle
+    mol = Mole(atom=geom.water_cluster(1, box=4.0, seed=2),
+               basis='standin-cc-pvdz').build()
+    opt = hf_oracle.VHFOpt(mol).build()
+    pm, C = opt.mol, opt.coeff
+    ao = pm.ao_loc_nr(cart=True)
+    n = ao[-1]
+    eri = np.zeros((n, n, n, n))
+    for i in range(pm.nbas):
+        for j in range(pm.nbas):
+            for k in range(pm.nbas):
+                for l in range(pm.nbas):
+                    eri[ao[i]:ao[i + 1], ao[j]:ao[j + 1], ao[k]:ao[k + 1],
+                        ao[l]:ao[l + 1]] = oracle.eri_shells(pm, i, j, k, l)
+    rng = np.random.default_rng(4)
+    d = rng.random((mol.nao, mol.nao))
+    d = d + d.T
+    w = C @ d @ C.T
+    rj = C.T @ np.einsum('ijkl,kl->ij', eri, w) @ C
+    rk = C.T @ np.einsum('ikjl,kl->ij', eri, w) @ C
+    vj, vk = hf_oracle.get_jk(mol, d, vhfopt=opt)
+    assert abs(vj - rj).max() <= 1e-11 * abs(rj).max()
+    assert abs(vk - rk).max() <= 1e-11 * abs(rk).max()
+
+
+@pytest.mark.parametrize('case', ['h2o-dz', 'h2o2-tzvp', 'walk6-631gs'])
+def test_oracle_reproduces_golden(case):
+    """The oracle against the committed fixtures (regression pin; the
+    fixtures and their generator are in tests/golden)."""
+    from oracle import hf_oracle
+    from tests.golden.make_golden import case_inputs
+    g = np.load(GOLDEN)
+    mol, dm = case_inputs(case)
+    vj, vk = hf_oracle.get_jk(mol, dm)
+    np.testing.assert_allclose(vj, g[case + '/vj'], rtol=0, atol=1e-12)
+    np.testing.assert_allclose(vk, g[case + '/vk'], rtol=0, atol=1e-12)
