@@ -70,6 +70,7 @@ struct jk_batch {
     int w_ndm = -1;
     // captured graph
     cudaGraphExec_t graph = nullptr;
+    JKFanout fan;  // side streams of the class launches
 };
 
 // per (molecule, gi, gj): max |D| over the group block (blockIdx.z = molecule)
@@ -131,6 +132,7 @@ __global__ void jk_symmetrize_batch_kernel(const JKSym* __restrict__ t, double f
 static void free_batch(jk_batch* t) {
     if (!t) return;
     if (t->graph) cudaGraphExecDestroy(t->graph);
+    t->fan.destroy();
     cudaFree(t->d_cq);
     cudaFree(t->d_dmc);
     cudaFree(t->d_seg64);
@@ -149,6 +151,7 @@ static void free_batch(jk_batch* t) {
 static int batch_create(jk_basis_t* const* bases, int nmol, jk_batch* t) {
     BCUDA(cudaGetDevice(&t->device));
     BCUDA(cudaDeviceGetAttribute(&t->nsm, cudaDevAttrMultiProcessorCount, t->device));
+    BCUDA(t->fan.init());
     t->nmol = nmol;
     std::vector<JKScreenCQ> cqs;
     std::map<std::tuple<int, int, int>, int> kidx;
@@ -297,17 +300,19 @@ extern "C" int jk_batch_build(jk_batch_t* t, const double* const* dms, double* c
         jk_seg_prefix_kernel<<<nkeys, 32, 0, st>>>(t->d_cnt32, t->d_key_off, t->d_segt32);
         BCUDA(cudaGetLastError());
     }
+    BCUDA(t->fan.begin(st));
     for (int k = 0; k < nkeys; k++) {
         const JKBatchKey& key = t->keys[k];
         int off = t->key_off[k], n = t->key_off[k + 1] - off;
         jk_launch_batch_fn f = jk_internal_batch_launcher(key.cls, 0);
-        BCUDA(f(t->d_seg64 + off, t->d_segt64 + off + k, n, key.max_tasks, t->nsm, st));
+        BCUDA(f(t->d_seg64 + off, t->d_segt64 + off + k, n, key.max_tasks, t->nsm, t->fan.pick(2 * k)));
         if (fp32_cutoff > 0) {
             jk_launch_batch_fn f32 = jk_internal_batch_launcher(key.cls, 1);
             if (!f32) return jk_internal_set_err(JK_ERR_UNSUPPORTED, "no FP32 kernel for a class");
-            BCUDA(f32(t->d_seg32 + off, t->d_segt32 + off + k, n, key.max_tasks, t->nsm, st));
+            BCUDA(f32(t->d_seg32 + off, t->d_segt32 + off + k, n, key.max_tasks, t->nsm, t->fan.pick(2 * k + 1)));
         }
     }
+    BCUDA(t->fan.end(st));
     return JK_OK;
 }
 

@@ -397,6 +397,7 @@ static void free_basis(jk_basis* b) {
     cudaFree(b->d_task01);
     cudaFree(b->d_work);
     cudaFree(b->d_pack);
+    b->fan.destroy();
     cudaFree(b->d_pk);
     if (b->h_qoff1) cudaFreeHost(b->h_qoff1);
     if (b->blas) cublasDestroy(b->blas);
@@ -671,6 +672,7 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
         b->h_pack.push_back(k);
     }
     CUDA_TRY(upload(&b->d_pack, b->h_pack.data(), b->h_pack.size()));
+    CUDA_TRY(b->fan.init());
     return JK_OK;
 }
 
@@ -798,6 +800,7 @@ extern "C" int jk_build(jk_basis_t* b, const double* dm, int n_dm, double* vj, d
         CUDA_TRY(cudaGetLastError());
         CUDA_TRY(cudaMemsetAsync(jp, 0, sizeof(double) * n_dm * b->pack_total, st));
     }
+    CUDA_TRY(b->fan.begin(st));
     for (int c = 0; c < b->ncq; c++) {
         const JKScreenCQ& cq = b->h_cq[c];
         JKSeg seg;
@@ -817,15 +820,16 @@ extern "C" int jk_build(jk_basis_t* b, const double* dm, int n_dm, double* vj, d
         int ci = class_index(b, cq.cp_ij, cq.cp_kl);
         jk_launch_fn fn = g_tab64[ci];
         if (!fn) return set_err(JK_ERR_UNSUPPORTED, "no kernel for class quartet %d", c);
-        CUDA_TRY(fn(seg, b->d_task0 + 2 * c, maxt, b->nsm, st));
+        CUDA_TRY(fn(seg, b->d_task0 + 2 * c, maxt, b->nsm, b->fan.pick(2 * c)));
         if (fp32_cutoff > 0) {
             jk_launch_fn f32 = g_tab32[ci];
             if (!f32) return set_err(JK_ERR_UNSUPPORTED, "no FP32 kernel for class quartet %d", c);
             seg.qoff = b->d_qoff32 + cq.qoff_off;
             seg.kl_base = b->d_klb + cq.qoff_off;
-            CUDA_TRY(f32(seg, b->d_task032 + 2 * c, maxt, b->nsm, st));
+            CUDA_TRY(f32(seg, b->d_task032 + 2 * c, maxt, b->nsm, b->fan.pick(2 * c + 1)));
         }
     }
+    CUDA_TRY(b->fan.end(st));
     if (packed) {
         jk_pack_kernel<<<pk_blocks, 256, 0, st>>>(b->d_pack, b->ncp, b->pack_total, b->d_pair2bra, b->d_pair2ket,
                                                    b->d_ao_loc, dm, b->nao, n_dm, nullptr, jp, vj, 1);

@@ -37,6 +37,51 @@ void jk_internal_fill_seg(const jk_basis_t* b, int cp_ij, int cp_kl, const long 
 int jk_internal_launch(const jk_basis_t* b, int cp_ij, int cp_kl, const JKSeg& seg, const long long* d_task0,
                        long long max_tasks, void* stream);
 
+// Side streams of the class launches.  Every class kernel adds into J and K
+// with atomics, so launches of different class quartets (and the FP64 and
+// FP32 parts of one) may run concurrently; spreading them over a few
+// streams overlaps the ramp-up and tail of the many small launches of a
+// build.  begin() forks from the caller's stream with an event, end() joins
+// back (both record into a CUDA graph when the caller's stream is captured).
+#define JK_SIDE_STREAMS 4
+struct JKFanout {
+    cudaStream_t s[JK_SIDE_STREAMS] = {};
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t join[JK_SIDE_STREAMS] = {};
+    cudaError_t init() {
+        cudaError_t e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+        for (int i = 0; e == cudaSuccess && i < JK_SIDE_STREAMS; i++) {
+            e = cudaStreamCreateWithFlags(&s[i], cudaStreamNonBlocking);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join[i], cudaEventDisableTiming);
+        }
+        return e;
+    }
+    cudaError_t begin(cudaStream_t st) {
+        cudaError_t e = cudaEventRecord(fork, st);
+        for (int i = 0; e == cudaSuccess && i < JK_SIDE_STREAMS; i++) e = cudaStreamWaitEvent(s[i], fork, 0);
+        return e;
+    }
+    cudaStream_t pick(int i) const { return s[i % JK_SIDE_STREAMS]; }
+    cudaError_t end(cudaStream_t st) {
+        cudaError_t e = cudaSuccess;
+        for (int i = 0; e == cudaSuccess && i < JK_SIDE_STREAMS; i++) {
+            e = cudaEventRecord(join[i], s[i]);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(st, join[i], 0);
+        }
+        return e;
+    }
+    void destroy() {
+        for (int i = 0; i < JK_SIDE_STREAMS; i++) {
+            if (s[i]) cudaStreamDestroy(s[i]);
+            if (join[i]) cudaEventDestroy(join[i]);
+            s[i] = nullptr;
+            join[i] = nullptr;
+        }
+        if (fork) cudaEventDestroy(fork);
+        fork = nullptr;
+    }
+};
+
 // one class pair in the pair-packed density / J buffers of jk_build
 struct JKPackCls {
     long long off;      // first packed element of the class
@@ -75,6 +120,7 @@ struct jk_basis {
     long long qoff1_cap = 0;
     long long* h_qoff1 = nullptr;  // pinned
     size_t h_qoff1_cap = 0;
+    JKFanout fan;  // side streams of the class launches
     // pair-packed J side of jk_build
     std::vector<JKPackCls> h_pack;
     JKPackCls* d_pack = nullptr;

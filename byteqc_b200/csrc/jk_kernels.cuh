@@ -168,6 +168,46 @@ __device__ __forceinline__ JKPrim jk_prim(const JKSeg& sg, int pij, int pkl) {
     return p;
 }
 
+// One primitive pair of a shell pair (exponent sum, its inverse, e12 / a12,
+// product centre).  The primitive loops load the ket side once per ket
+// primitive pair and pair it with every bra primitive pair (the bra side is
+// the same for the lanes of a warp, a broadcast from L1), instead of
+// reloading both sides for every primitive quartet.
+struct JKPP {
+    double a, ia, e, P[3];
+};
+
+__device__ __forceinline__ JKPP jk_pp(const JKSeg& sg, int p) {
+    JKPP r;
+    r.a = __ldg(sg.a12 + p);
+    r.ia = __ldg(sg.ia12 + p);
+    r.e = __ldg(sg.e12 + p) * r.ia;
+    r.P[0] = __ldg(sg.x12 + p);
+    r.P[1] = __ldg(sg.y12 + p);
+    r.P[2] = __ldg(sg.z12 + p);
+    return r;
+}
+
+__device__ __forceinline__ JKPrim jk_prim2(const JKPP& b, const JKPP& k) {
+    JKPrim p;
+    p.A = b.a;
+    p.B = k.a;
+    p.iA = b.ia;
+    p.iB = k.ia;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        p.P[d] = b.P[d];
+        p.Q[d] = k.P[d];
+    }
+    p.AB = p.A + p.B;
+    p.iAB = 1. / p.AB;
+    const double rho = p.A * p.B * p.iAB;
+    const double dx = p.P[0] - p.Q[0], dy = p.P[1] - p.Q[1], dz = p.P[2] - p.Q[2];
+    p.x = rho * (dx * dx + dy * dy + dz * dz);
+    p.sy = b.e * k.e * sqrt(p.iAB);
+    return p;
+}
+
 // build the 2D block of (axis d, root r) into out
 template <class C, typename R, typename OutT>
 __device__ __forceinline__ void jk_unit(const JKPrim& p, double s, double w, int d, double norm, const double* ri,
@@ -220,6 +260,42 @@ __device__ __forceinline__ JKPrimF jk_prim_f(const JKSeg& sg, int pij, int pkl, 
     p.iAB = rs * rs;
     p.x = p.A * p.B * p.iAB * (p.PQ[0] * p.PQ[0] + p.PQ[1] * p.PQ[1] + p.PQ[2] * p.PQ[2]);
     p.sy = E * rs;  // e12 e12' / (A B sqrt(A + B))
+    return p;
+}
+
+// single-precision primitive pair: a12, 1/a12, e12/a12, P - R of its first shell
+struct JKPPF {
+    float a, ia, e, D[3];
+};
+
+__device__ __forceinline__ JKPPF jk_ppf(const JKSeg& sg, int p) {
+    const float* f = sg.pf;
+    const long long n = sg.npf;
+    JKPPF r;
+    r.a = __ldg(f + p);
+    r.ia = __ldg(f + n + p);
+    r.e = __ldg(f + 2 * n + p);
+#pragma unroll
+    for (int d = 0; d < 3; d++) r.D[d] = __ldg(f + (3 + d) * n + p);
+    return r;
+}
+
+__device__ __forceinline__ JKPrimF jk_prim_f2(const JKPPF& b, const JKPPF& k, const float* ac) {
+    JKPrimF p;
+    p.A = b.a;
+    p.B = k.a;
+    p.iA = b.ia;
+    p.iB = k.ia;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        p.PA[d] = b.D[d];
+        p.QC[d] = k.D[d];
+        p.PQ[d] = (p.PA[d] - p.QC[d]) + ac[d];
+    }
+    const float rs = rsqrtf(p.A + p.B);
+    p.iAB = rs * rs;
+    p.x = p.A * p.B * p.iAB * (p.PQ[0] * p.PQ[0] + p.PQ[1] * p.PQ[1] + p.PQ[2] * p.PQ[2]);
+    p.sy = b.e * k.e * rs;
     return p;
 }
 
@@ -472,9 +548,13 @@ __device__ __forceinline__ void jk_thread_pass(const JKSeg& sg, const JKQuartet&
             ac[d] = (float)(ri[d] - rk[d]);
         }
         const float normf = (float)q.norm;
-        for (int ip = 0; ip < sg.nprim_ij; ip++)
-            for (int kp = 0; kp < sg.nprim_kl; kp++) {
-                JKPrimF p = jk_prim_f(sg, q.prim_ij + ip, q.prim_kl + kp, ac);
+        const int npij = sg.nprim_ij, npkl = sg.nprim_kl;
+        JKPPF kn = jk_ppf(sg, q.prim_kl);
+        for (int kp = 0; kp < npkl; kp++) {
+            const JKPPF kc = kn;
+            if (kp + 1 < npkl) kn = jk_ppf(sg, q.prim_kl + kp + 1);  // next ket primitive, in flight
+            for (int ip = 0; ip < npij; ip++) {
+                JKPrimF p = jk_prim_f2(jk_ppf(sg, q.prim_ij + ip), kc, ac);
                 float rs[NR], rw[NR];
                 rys_roots_all_f<NR>(tabf, p.x, rs, rw);
 #pragma unroll
@@ -486,10 +566,15 @@ __device__ __forceinline__ void jk_thread_pass(const JKSeg& sg, const JKQuartet&
                     jk_thread_products<C, R, CI0, NI>(acc, Ix, Iy, Iz);
                 }
             }
+        }
     } else {
-        for (int ip = 0; ip < sg.nprim_ij; ip++)
-            for (int kp = 0; kp < sg.nprim_kl; kp++) {
-                JKPrim p = jk_prim(sg, q.prim_ij + ip, q.prim_kl + kp);
+        const int npij = sg.nprim_ij, npkl = sg.nprim_kl;
+        JKPP kn = jk_pp(sg, q.prim_kl);
+        for (int kp = 0; kp < npkl; kp++) {
+            const JKPP kc = kn;
+            if (kp + 1 < npkl) kn = jk_pp(sg, q.prim_kl + kp + 1);  // next ket primitive, in flight
+            for (int ip = 0; ip < npij; ip++) {
+                JKPrim p = jk_prim2(jk_pp(sg, q.prim_ij + ip), kc);
                 double rs[NR], rw[NR];
                 rys_roots_all<NR>(tab, p.x, rs, rw);
 #pragma unroll
@@ -502,6 +587,7 @@ __device__ __forceinline__ void jk_thread_pass(const JKSeg& sg, const JKQuartet&
                     jk_thread_products<C, R, CI0, NI>(acc, Ix, Iy, Iz);
                 }
             }
+        }
     }
     jk_thread_digest<C, R, NI>(sg, q, CI0, acc, sink);
 }
@@ -682,10 +768,12 @@ __device__ __forceinline__ void jk_team_body(const Src& src) {
         R acc[C::NACC];
 #pragma unroll
         for (int e = 0; e < C::NACC; e++) acc[e] = R(0);
-        for (int ip = 0; ip < nprim_ij; ip++)
-            for (int kp = 0; kp < nprim_kl; kp++) {
+        for (int kp = 0; kp < nprim_kl; kp++) {
+            JKPP kc;
+            if (active) kc = jk_pp(sg, q.prim_kl + kp);
+            for (int ip = 0; ip < nprim_ij; ip++) {
                 if (active) {
-                    JKPrim p = jk_prim(sg, q.prim_ij + ip, q.prim_kl + kp);
+                    JKPrim p = jk_prim2(jk_pp(sg, q.prim_ij + ip), kc);
                     for (int u = lane; u < 3 * NR; u += T) {
                         int r = u / 3, d = u - 3 * r;
                         double s, w;
@@ -729,6 +817,7 @@ __device__ __forceinline__ void jk_team_body(const Src& src) {
                 }
                 __syncthreads();
             }
+        }
 
         // ---- digestion ----
         // Outputs a thread owns completely go to buf; the others are written as
