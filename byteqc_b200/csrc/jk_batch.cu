@@ -71,6 +71,13 @@ struct jk_batch {
     // captured graph
     cudaGraphExec_t graph = nullptr;
     JKFanout fan;  // side streams of the class launches
+    // pair-packed J side: every molecule's packed densities, then every
+    // molecule's packed J accumulators (one memset clears them all)
+    double* d_pk = nullptr;
+    size_t pk_cap = 0, pk_jp = 0;  // capacity; first accumulator element
+    JKPackMol* d_pmol = nullptr;
+    long long pk_max = 0;          // largest per-molecule packed size
+    bool packed = false;
 };
 
 // per (molecule, gi, gj): max |D| over the group block (blockIdx.z = molecule)
@@ -133,6 +140,8 @@ static void free_batch(jk_batch* t) {
     if (!t) return;
     if (t->graph) cudaGraphExecDestroy(t->graph);
     t->fan.destroy();
+    cudaFree(t->d_pk);
+    cudaFree(t->d_pmol);
     cudaFree(t->d_cq);
     cudaFree(t->d_dmc);
     cudaFree(t->d_seg64);
@@ -244,6 +253,35 @@ static int batch_segments(jk_batch* t, const double* const* dms, double* const* 
         same = t->seg_dm[m] == dms[m] && t->seg_vj[m] == (vjs ? vjs[m] : nullptr) &&
                t->seg_vk[m] == (vks ? vks[m] : nullptr);
     if (same) return JK_OK;
+    // earlier launches may still read the old tables and buffers
+    BCUDA(cudaStreamSynchronize(st));
+    // pair-packed J side (with J only)
+    t->packed = vjs != nullptr;
+    std::vector<size_t> dp_off(t->nmol, 0);
+    t->pk_max = 0;
+    if (t->packed) {
+        size_t tot = 0;
+        for (int m = 0; m < t->nmol; m++) {
+            dp_off[m] = tot;
+            tot += (size_t)n_dm * t->mols[m]->pack_total;
+            t->pk_max = std::max(t->pk_max, t->mols[m]->pack_total);
+        }
+        t->pk_jp = tot;
+        if (2 * tot > t->pk_cap) {
+            cudaFree(t->d_pk);
+            t->d_pk = nullptr;
+            BCUDA(cudaMalloc(&t->d_pk, sizeof(double) * std::max<size_t>(2 * tot, 1)));
+            t->pk_cap = 2 * tot;
+        }
+        std::vector<JKPackMol> pm(t->nmol);
+        for (int m = 0; m < t->nmol; m++) {
+            const jk_basis* b = t->mols[m];
+            pm[m] = JKPackMol{b->d_pack, b->ncp, b->pack_total, b->d_pair2bra, b->d_pair2ket, b->d_ao_loc,
+                              dms[m], b->nao, n_dm, t->d_pk + dp_off[m], t->d_pk + tot + dp_off[m], vjs[m]};
+        }
+        if (!t->d_pmol) BCUDA(cudaMalloc(&t->d_pmol, sizeof(JKPackMol) * t->nmol));
+        BCUDA(cudaMemcpy(t->d_pmol, pm.data(), sizeof(JKPackMol) * t->nmol, cudaMemcpyHostToDevice));
+    }
     std::vector<JKSeg> s64(std::max(1, t->nseg)), s32(std::max(1, t->nseg));
     int i = 0;
     for (auto& k : t->keys)
@@ -253,6 +291,22 @@ static int batch_segments(jk_batch* t, const double* const* dms, double* const* 
                                        vks ? vks[m] : nullptr, 0, &s64[i]);
             jk_internal_fill_seg_batch(t->mols[m], sgi.second, dms[m], n_dm, vjs ? vjs[m] : nullptr,
                                        vks ? vks[m] : nullptr, 1, &s32[i]);
+            if (t->packed) {
+                const jk_basis* b = t->mols[m];
+                const JKScreenCQ& cq = b->h_cq[sgi.second];
+                const JKPackCls &ki = b->h_pack[cq.cp_ij], &kk = b->h_pack[cq.cp_kl];
+                double* dp = t->d_pk + dp_off[m];
+                double* jp = t->d_pk + t->pk_jp + dp_off[m];
+                for (JKSeg* sg : {&s64[i], &s32[i]}) {
+                    sg->dp_ij = dp + ki.off;
+                    sg->dp_kl = dp + kk.off;
+                    sg->jp_ij = jp + ki.off;
+                    sg->jp_kl = jp + kk.off;
+                    sg->np_ij = ki.np;
+                    sg->np_kl = kk.np;
+                    sg->pk_stride = b->pack_total;
+                }
+            }
             i++;
         }
     t->h_dmc.resize(t->nmol);
@@ -260,8 +314,6 @@ static int batch_segments(jk_batch* t, const double* const* dms, double* const* 
         jk_basis* b = t->mols[m];
         t->h_dmc[m] = JKDmCond{dms[m], b->d_group_ao, b->d_dm_cond, b->nao, n_dm, b->ngroups};
     }
-    // earlier launches may still read the old tables
-    BCUDA(cudaStreamSynchronize(st));
     BCUDA(cudaMemcpy(t->d_seg64, s64.data(), sizeof(JKSeg) * t->nseg, cudaMemcpyHostToDevice));
     BCUDA(cudaMemcpy(t->d_seg32, s32.data(), sizeof(JKSeg) * t->nseg, cudaMemcpyHostToDevice));
     BCUDA(cudaMemcpy(t->d_dmc, t->h_dmc.data(), sizeof(JKDmCond) * t->nmol, cudaMemcpyHostToDevice));
@@ -300,6 +352,11 @@ extern "C" int jk_batch_build(jk_batch_t* t, const double* const* dms, double* c
         jk_seg_prefix_kernel<<<nkeys, 32, 0, st>>>(t->d_cnt32, t->d_key_off, t->d_segt32);
         BCUDA(cudaGetLastError());
     }
+    if (t->packed) {
+        rc = jk_internal_pack_batch(t->d_pmol, t->nmol, t->pk_max, 0, stream);
+        if (rc) return rc;
+        BCUDA(cudaMemsetAsync(t->d_pk + t->pk_jp, 0, sizeof(double) * t->pk_jp, st));
+    }
     BCUDA(t->fan.begin(st));
     for (int k = 0; k < nkeys; k++) {
         const JKBatchKey& key = t->keys[k];
@@ -313,6 +370,10 @@ extern "C" int jk_batch_build(jk_batch_t* t, const double* const* dms, double* c
         }
     }
     BCUDA(t->fan.end(st));
+    if (t->packed) {
+        rc = jk_internal_pack_batch(t->d_pmol, t->nmol, t->pk_max, 1, stream);
+        if (rc) return rc;
+    }
     return JK_OK;
 }
 

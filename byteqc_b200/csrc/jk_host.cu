@@ -327,11 +327,11 @@ __global__ void jk_screen_kernel(const JKScreenCQ* __restrict__ cqs, double tol,
 // every pair into dp (element c of pair p of class k at off_k + c*np_k + p,
 // one copy per density); mode 1: add the packed J accumulators jp into vj.
 // Every (pair, component) is a distinct element of D and of vj.
-__global__ void jk_pack_kernel(const JKPackCls* __restrict__ cls, int ncls, long long total,
-                               const int* __restrict__ pair2bra, const int* __restrict__ pair2ket,
-                               const int* __restrict__ ao_loc, const double* __restrict__ dm, int nao, int n_dm,
-                               double* __restrict__ dp, const double* __restrict__ jp, double* __restrict__ vj,
-                               int mode) {
+__device__ __forceinline__ void jk_pack_body(const JKPackCls* __restrict__ cls, int ncls, long long total,
+                                             const int* __restrict__ pair2bra, const int* __restrict__ pair2ket,
+                                             const int* __restrict__ ao_loc, const double* __restrict__ dm, int nao,
+                                             int n_dm, double* __restrict__ dp, const double* __restrict__ jp,
+                                             double* __restrict__ vj, int mode) {
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
         int lo = 0, hi = ncls - 1;
@@ -351,6 +351,22 @@ __global__ void jk_pack_kernel(const JKPackCls* __restrict__ cls, int ncls, long
             else vj[mo + e] += jp[m * total + t];
         }
     }
+}
+
+__global__ void jk_pack_kernel(const JKPackCls* __restrict__ cls, int ncls, long long total,
+                               const int* __restrict__ pair2bra, const int* __restrict__ pair2ket,
+                               const int* __restrict__ ao_loc, const double* __restrict__ dm, int nao, int n_dm,
+                               double* __restrict__ dp, const double* __restrict__ jp, double* __restrict__ vj,
+                               int mode) {
+    jk_pack_body(cls, ncls, total, pair2bra, pair2ket, ao_loc, dm, nao, n_dm, dp, jp, vj, mode);
+}
+
+// one molecule per blockIdx.y
+__global__ void jk_pack_batch_kernel(const JKPackMol* __restrict__ mols, int mode) {
+    const JKPackMol m = mols[blockIdx.y];
+    if (m.total <= 0) return;
+    jk_pack_body(m.cls, m.ncls, m.total, m.pair2bra, m.pair2ket, m.ao_loc, m.dm, m.nao, m.n_dm, m.dp, m.jp, m.vj,
+                 mode);
 }
 
 // J = 2 (V + V^T), K = V + V^T in place on the working-basis buffers, where
@@ -1150,6 +1166,14 @@ void jk_internal_fill_seg_batch(const jk_basis_t* b, int c, const double* dm, in
     const JKScreenCQ& cq = b->h_cq[c];
     fill_seg(b, cq.cp_ij, cq.cp_kl, fp32 ? cq.qoff32 : cq.qoff, cq.n_ij, dm, n_dm, vj, vk, out);
     if (fp32) out->kl_base = cq.klb;
+}
+
+int jk_internal_pack_batch(const JKPackMol* d_mols, int nmol, long long max_total, int mode, void* stream) {
+    if (nmol <= 0 || max_total <= 0) return JK_OK;
+    const unsigned bx = (unsigned)std::min<long long>((max_total + 255) / 256, 64);
+    jk_pack_batch_kernel<<<dim3(bx, nmol), 256, 0, (cudaStream_t)stream>>>(d_mols, mode);
+    CUDA_TRY(cudaGetLastError());
+    return JK_OK;
 }
 
 int jk_internal_screen(const JKScreenCQ* d_cq, int ncq, double tol, int nbins, int prescreen, double fp32_cutoff,

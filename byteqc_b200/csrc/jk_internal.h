@@ -43,7 +43,7 @@ int jk_internal_launch(const jk_basis_t* b, int cp_ij, int cp_kl, const JKSeg& s
 // streams overlaps the ramp-up and tail of the many small launches of a
 // build.  begin() forks from the caller's stream with an event, end() joins
 // back (both record into a CUDA graph when the caller's stream is captured).
-#define JK_SIDE_STREAMS 4
+#define JK_SIDE_STREAMS 8
 struct JKFanout {
     cudaStream_t s[JK_SIDE_STREAMS] = {};
     cudaEvent_t fork = nullptr;
@@ -87,6 +87,19 @@ struct JKPackCls {
     long long off;      // first packed element of the class
     int np, nfi, nfj;   // pairs, Cartesian components of the two shells
     int pair0;          // first pair of the class
+};
+
+// one molecule of a batched pack / unpack of the pair-packed J side
+struct JKPackMol {
+    const JKPackCls* cls;
+    int ncls;
+    long long total;
+    const int *pair2bra, *pair2ket, *ao_loc;
+    const double* dm;
+    int nao, n_dm;
+    double* dp;        // mode 0 output
+    const double* jp;  // mode 1 input
+    double* vj;        // mode 1 output
 };
 
 // Per-geometry state (opaque to callers of the C-ABI)
@@ -138,5 +151,7 @@ int jk_internal_class_index(const jk_basis_t* b, int cp_ij, int cp_kl);
 jk_launch_batch_fn jk_internal_batch_launcher(int class_idx, int fp32);
 void jk_internal_fill_seg_batch(const jk_basis_t* b, int c, const double* dm, int n_dm, double* vj, double* vk,
                                 int fp32, JKSeg* out);
+// pack (mode 0) or unpack (mode 1) the J side of nmol molecules (device table)
+int jk_internal_pack_batch(const JKPackMol* d_mols, int nmol, long long max_total, int mode, void* stream);
 int jk_internal_screen(const JKScreenCQ* d_cq, int ncq, double tol, int nbins, int prescreen, double fp32_cutoff,
                        void* stream);

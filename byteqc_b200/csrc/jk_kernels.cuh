@@ -147,27 +147,6 @@ struct JKPrim {
     double P[3], Q[3];
 };
 
-__device__ __forceinline__ JKPrim jk_prim(const JKSeg& sg, int pij, int pkl) {
-    JKPrim p;
-    p.A = __ldg(sg.a12 + pij);
-    p.B = __ldg(sg.a12 + pkl);
-    p.P[0] = __ldg(sg.x12 + pij);
-    p.P[1] = __ldg(sg.y12 + pij);
-    p.P[2] = __ldg(sg.z12 + pij);
-    p.Q[0] = __ldg(sg.x12 + pkl);
-    p.Q[1] = __ldg(sg.y12 + pkl);
-    p.Q[2] = __ldg(sg.z12 + pkl);
-    p.iA = __ldg(sg.ia12 + pij);
-    p.iB = __ldg(sg.ia12 + pkl);
-    p.AB = p.A + p.B;
-    p.iAB = 1. / p.AB;
-    double rho = p.A * p.B * p.iAB;
-    double dx = p.P[0] - p.Q[0], dy = p.P[1] - p.Q[1], dz = p.P[2] - p.Q[2];
-    p.x = rho * (dx * dx + dy * dy + dz * dz);
-    p.sy = __ldg(sg.e12 + pij) * __ldg(sg.e12 + pkl) * p.iA * p.iB * sqrt(p.iAB);
-    return p;
-}
-
 // One primitive pair of a shell pair (exponent sum, its inverse, e12 / a12,
 // product centre).  The primitive loops load the ket side once per ket
 // primitive pair and pair it with every bra primitive pair (the bra side is
@@ -240,28 +219,6 @@ struct JKPrimF {
     float x, A, B, iA, iB, iAB, sy;
     float PA[3], QC[3], PQ[3];
 };
-
-__device__ __forceinline__ JKPrimF jk_prim_f(const JKSeg& sg, int pij, int pkl, const float* ac) {
-    const float* f = sg.pf;
-    const long long n = sg.npf;
-    JKPrimF p;
-    p.A = __ldg(f + pij);
-    p.B = __ldg(f + pkl);
-    p.iA = __ldg(f + n + pij);
-    p.iB = __ldg(f + n + pkl);
-    const float E = __ldg(f + 2 * n + pij) * __ldg(f + 2 * n + pkl);
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-        p.PA[d] = __ldg(f + (3 + d) * n + pij);
-        p.QC[d] = __ldg(f + (3 + d) * n + pkl);
-        p.PQ[d] = (p.PA[d] - p.QC[d]) + ac[d];
-    }
-    const float rs = rsqrtf(p.A + p.B);
-    p.iAB = rs * rs;
-    p.x = p.A * p.B * p.iAB * (p.PQ[0] * p.PQ[0] + p.PQ[1] * p.PQ[1] + p.PQ[2] * p.PQ[2]);
-    p.sy = E * rs;  // e12 e12' / (A B sqrt(A + B))
-    return p;
-}
 
 // single-precision primitive pair: a12, 1/a12, e12/a12, P - R of its first shell
 struct JKPPF {
@@ -616,6 +573,15 @@ __device__ __forceinline__ void jk_thread_quartet(const JKSeg& sg, const JKQuart
     jk_thread_passes<C, R, 0>(sg, q, tab, ri, rj, rk, rl, sink);
 }
 
+// Resident 128-thread blocks asked of the register allocator (single-segment
+// kernel).  The FP32 quartets hold half-width values and spend more of their
+// time waiting on loads, so they get more resident warps; the batched kernel
+// keeps C::MINB (its segment cursor would spill).
+template <class C, typename R>
+struct JKThreadMinBlocks {
+    static constexpr int value = sizeof(R) == 4 ? (C::W <= 24 ? 8 : (C::W <= 40 ? 6 : 4)) : C::MINB;
+};
+
 template <class C, typename R, class Src>
 __device__ __forceinline__ void jk_thread_body(const Src& src, double* jk_tab) {
     if constexpr (JKF32Prim<C, R>::value)
@@ -644,7 +610,7 @@ __device__ __forceinline__ void jk_thread_body(const Src& src, double* jk_tab) {
 }
 
 template <class C, typename R>
-__global__ void __launch_bounds__(128, C::MINB) jk_thread_kernel(const __grid_constant__ JKSeg sg,
+__global__ void __launch_bounds__(128, (JKThreadMinBlocks<C, R>::value)) jk_thread_kernel(const __grid_constant__ JKSeg sg,
                                                                  const long long* __restrict__ task0) {
     extern __shared__ __align__(16) double jk_tab[];
     JKOneSeg src{sg, task0};
