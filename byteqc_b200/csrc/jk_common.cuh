@@ -430,6 +430,13 @@ struct JKSeg {
     // mode, SoA of npf floats each: a12 | 1/a12 | e12/a12 | P - R_bra (x, y, z)
     const float* pf;
     long long npf;
+    // pair geometry, indexed by pair (stride npt): the centres of the pair's
+    // two shells (SoA x_a y_a z_a x_b y_b z_b) and their first AOs (SoA
+    // ao_a ao_b); one dependent load per quartet side instead of two, and
+    // coalesced on the ket side (consecutive lanes hold consecutive pairs)
+    const double* pgeo;
+    const int* pao;
+    int npt;
     const double* bas_x;  // shell centres, SoA x[nbas], y[nbas], z[nbas]
     int nbas;
     const int* ao_loc;

@@ -413,6 +413,8 @@ static void free_basis(jk_basis* b) {
     cudaFree(b->d_task01);
     cudaFree(b->d_work);
     cudaFree(b->d_pack);
+    cudaFree(b->d_pgeo);
+    cudaFree(b->d_pao);
     b->fan.destroy();
     cudaFree(b->d_pk);
     if (b->h_qoff1) cudaFreeHost(b->h_qoff1);
@@ -627,6 +629,21 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
     }
     CUDA_TRY(upload(&b->d_prim, prim.data(), prim.size()));
     CUDA_TRY(upload(&b->d_primf, primf.data(), primf.size()));
+    {
+        // pair geometry: the two shells' centres and first AOs per pair
+        const size_t np = b->h_pair2bra.size();
+        std::vector<double> geo(6 * (np ? np : 1));
+        std::vector<int> pao(2 * (np ? np : 1));
+        for (size_t p = 0; p < np; p++) {
+            const int sh[2] = {b->h_pair2bra[p], b->h_pair2ket[p]};
+            for (int a = 0; a < 2; a++) {
+                for (int d = 0; d < 3; d++) geo[(3 * a + d) * np + p] = bx[(size_t)d * nbas + sh[a]];
+                pao[a * np + p] = b->h_ao_loc[sh[a]];
+            }
+        }
+        CUDA_TRY(upload(&b->d_pgeo, geo.data(), geo.size()));
+        CUDA_TRY(upload(&b->d_pao, pao.data(), pao.size()));
+    }
     CUDA_TRY(upload(&b->d_pair2bra, b->h_pair2bra.data(), b->h_pair2bra.size()));
     CUDA_TRY(upload(&b->d_pair2ket, b->h_pair2ket.data(), b->h_pair2ket.size()));
     CUDA_TRY(upload(&b->d_log_q, b->h_log_q.data(), b->h_log_q.size()));
@@ -764,6 +781,9 @@ static void fill_seg(const jk_basis* b, int cp_ij, int cp_kl, const long long* q
     s->pf = b->d_primf;
     s->npf = n;
     s->bas_x = b->d_bas_x;
+    s->pgeo = b->d_pgeo;
+    s->pao = b->d_pao;
+    s->npt = (int)b->h_pair2bra.size();
     s->nbas = b->nbas;
     s->ao_loc = b->d_ao_loc;
     s->dm = dm;

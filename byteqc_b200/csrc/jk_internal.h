@@ -134,6 +134,8 @@ struct jk_basis {
     long long* h_qoff1 = nullptr;  // pinned
     size_t h_qoff1_cap = 0;
     JKFanout fan;  // side streams of the class launches
+    double* d_pgeo = nullptr;  // pair geometry (JKSeg::pgeo)
+    int* d_pao = nullptr;      // first AOs of the pair's shells (JKSeg::pao)
     // pair-packed J side of jk_build
     std::vector<JKPackCls> h_pack;
     JKPackCls* d_pack = nullptr;

@@ -43,7 +43,8 @@ __device__ __forceinline__ int jk_find_row(const long long* __restrict__ qoff, i
 }
 
 struct JKQuartet {
-    int ish, jsh, ksh, lsh;
+    int bij, bkl;          // global pair indices
+    int i0, j0, k0, l0;    // first AO of each shell
     int prim_ij, prim_kl;  // first primitive pair of ij and kl
     int row, col;          // pair indices within the two classes
     double norm;
@@ -52,11 +53,13 @@ struct JKQuartet {
 __device__ __forceinline__ JKQuartet jk_quartet_at(const JKSeg& sg, int row, int col) {
     JKQuartet q;
     if (sg.kl_base) col += __ldg(sg.kl_base + row);
-    int bij = sg.pair_ij0 + row, bkl = sg.pair_kl0 + col;
-    q.ish = __ldg(sg.pair2bra + bij);
-    q.jsh = __ldg(sg.pair2ket + bij);
-    q.ksh = __ldg(sg.pair2bra + bkl);
-    q.lsh = __ldg(sg.pair2ket + bkl);
+    const int bij = sg.pair_ij0 + row, bkl = sg.pair_kl0 + col;
+    q.bij = bij;
+    q.bkl = bkl;
+    q.i0 = __ldg(sg.pao + bij);
+    q.j0 = __ldg(sg.pao + sg.npt + bij);
+    q.k0 = __ldg(sg.pao + bkl);
+    q.l0 = __ldg(sg.pao + sg.npt + bkl);
     q.prim_ij = sg.prim_ij0 + row * sg.nprim_ij;
     q.prim_kl = sg.prim_kl0 + col * sg.nprim_kl;
     q.row = row;
@@ -278,10 +281,13 @@ struct JKF32Prim {
     static constexpr bool value = sizeof(R) == 4 && C::NROOTS <= JK_F32_ROOTS;
 };
 
-__device__ __forceinline__ void load_center(const JKSeg& sg, int sh, double* r) {
-    r[0] = __ldg(sg.bas_x + sh);
-    r[1] = __ldg(sg.bas_x + sg.nbas + sh);
-    r[2] = __ldg(sg.bas_x + 2 * sg.nbas + sh);
+// centres of the two shells of pair p
+__device__ __forceinline__ void load_pair_centres(const JKSeg& sg, int p, double* ra, double* rb) {
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        ra[d] = __ldg(sg.pgeo + (size_t)d * sg.npt + p);
+        rb[d] = __ldg(sg.pgeo + (size_t)(3 + d) * sg.npt + p);
+    }
 }
 
 // D_ab with the reference's index convention dm[a + nao*b]
@@ -330,19 +336,19 @@ template <class C, typename R, int NI, class Sink>
 __device__ __forceinline__ void jk_thread_digest(const JKSeg& sg, const JKQuartet& q, int CI0, const R* acc,
                                                  const Sink& sink) {
     const int nao = sg.nao;
-    const int i0 = __ldg(sg.ao_loc + q.ish) + CI0, j0 = __ldg(sg.ao_loc + q.jsh);
-    const int k0 = __ldg(sg.ao_loc + q.ksh), l0 = __ldg(sg.ao_loc + q.lsh);
+    const int i0 = q.i0 + CI0, j0 = q.j0;
+    const int k0 = q.k0, l0 = q.l0;
     // the lanes of a warp usually share the ij pair (consecutive kl of one
     // row): then the J_ij block is summed over the warp before it is added.
-    // In a batched launch a warp can straddle two molecules whose shells
+    // In a batched launch a warp can straddle two molecules whose pairs
     // carry the same indices, so the lanes must also share the output.
     const unsigned am = __activemask();
     bool wsame = false;
     if (am == 0xffffffffu) {
         const unsigned long long out = (unsigned long long)(sg.jp_ij ? (const void*)sg.jp_ij : (const void*)sg.vj);
-        int i_0 = __shfl_sync(am, q.ish, 0), j_0 = __shfl_sync(am, q.jsh, 0);
+        const int p_0 = __shfl_sync(am, q.bij, 0);
         unsigned long long o_0 = __shfl_sync(am, out, 0);
-        wsame = __all_sync(am, q.ish == i_0 && q.jsh == j_0 && out == o_0);
+        wsame = __all_sync(am, q.bij == p_0 && out == o_0);
     }
 #define ACC(i, j, k, l) ((double)acc[(((i) * C::NFJ + (j)) * C::NFK + (k)) * C::NFL + (l)])
     for (int idm = 0; idm < sg.n_dm; idm++) {
@@ -566,10 +572,8 @@ template <class C, typename R, class Sink>
 __device__ __forceinline__ void jk_thread_quartet(const JKSeg& sg, const JKQuartet& q, const double* __restrict__ tab,
                                                   const Sink& sink) {
     double ri[3], rj[3], rk[3], rl[3];
-    load_center(sg, q.ish, ri);
-    load_center(sg, q.jsh, rj);
-    load_center(sg, q.ksh, rk);
-    load_center(sg, q.lsh, rl);
+    load_pair_centres(sg, q.bij, ri, rj);
+    load_pair_centres(sg, q.bkl, rk, rl);
     jk_thread_passes<C, R, 0>(sg, q, tab, ri, rj, rk, rl, sink);
 }
 
@@ -726,10 +730,8 @@ __device__ __forceinline__ void jk_team_body(const Src& src) {
         }
         const JKSeg& sg = *sgp;
         if (active) {
-            load_center(sg, q.ish, ri);
-            load_center(sg, q.jsh, rj);
-            load_center(sg, q.ksh, rk);
-            load_center(sg, q.lsh, rl);
+            load_pair_centres(sg, q.bij, ri, rj);
+            load_pair_centres(sg, q.bkl, rk, rl);
         }
         R acc[C::NACC];
 #pragma unroll
@@ -795,8 +797,8 @@ __device__ __forceinline__ void jk_team_body(const Src& src) {
             double* mine = part + (size_t)lane * S::PSTRIDE;
             if (active) {
                 const int nao = sg.nao;
-                const int i0 = __ldg(sg.ao_loc + q.ish), j0 = __ldg(sg.ao_loc + q.jsh);
-                const int k0 = __ldg(sg.ao_loc + q.ksh), l0 = __ldg(sg.ao_loc + q.lsh);
+                const int i0 = q.i0, j0 = q.j0;
+                const int k0 = q.k0, l0 = q.l0;
                 const double* D = sg.dm + (size_t)idm * nao * nao;
                 if (C::P == 1) {
 #define A1(j, k, l) ((double)acc[((j) * C::NFK + (k)) * C::NFL + (l)])
@@ -969,8 +971,8 @@ __device__ __forceinline__ void jk_team_body(const Src& src) {
             __syncthreads();
             if (active) {  // flush the team's blocks to global memory
                 const int nao = sg.nao;
-                const int i0 = __ldg(sg.ao_loc + q.ish), j0 = __ldg(sg.ao_loc + q.jsh);
-                const int k0 = __ldg(sg.ao_loc + q.ksh), l0 = __ldg(sg.ao_loc + q.lsh);
+                const int i0 = q.i0, j0 = q.j0;
+                const int k0 = q.k0, l0 = q.l0;
                 const size_t moff = (size_t)idm * nao * nao;
                 for (int e = lane; e < S::BWORDS_RAW; e += T) {  // not the padding word
                     double v = buf[e];
