@@ -437,6 +437,9 @@ struct JKSeg {
     const double* pgeo;
     const int* pao;
     int npt;
+    // per pair: its leading primitive pairs that pass the exponent cutoff
+    // (the thread kernels loop over those only), or null
+    const int* pnp;
     const double* bas_x;  // shell centres, SoA x[nbas], y[nbas], z[nbas]
     int nbas;
     const int* ao_loc;

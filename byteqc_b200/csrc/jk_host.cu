@@ -17,6 +17,10 @@
 #include "jk_launch.cuh"
 #include "jk_internal.h"
 
+// primitive-pair screen of the thread kernels: exp(-mu r^2) below exp(-60)
+// (the default exponent cutoff of libcint's pair data) contributes nothing
+#define JK_PRIM_EXPCUT 60.0
+
 // ---------------------------------------------------------------------------
 // errors
 // ---------------------------------------------------------------------------
@@ -414,6 +418,7 @@ static void free_basis(jk_basis* b) {
     cudaFree(b->d_work);
     cudaFree(b->d_pack);
     cudaFree(b->d_pgeo);
+    cudaFree(b->d_pnp);
     cudaFree(b->d_pao);
     b->fan.destroy();
     cudaFree(b->d_pk);
@@ -592,6 +597,7 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
     // product centre is stored relative to the bra shell's centre so that
     // the small differences P - R_i keep their relative precision
     std::vector<float> primf(6 * (size_t)(npp ? npp : 1));
+    b->h_pnp.assign(std::max<size_t>(b->h_pair2bra.size(), 1), 0);
     {
         long long off = 0;
         for (size_t p = 0; p < b->h_pair2bra.size(); p++) {
@@ -607,8 +613,22 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
             double norm = common_fac_sp(li) * common_fac_sp(lj);
             double dx = ri[0] - rj[0], dy = ri[1] - rj[1], dz = ri[2] - rj[2];
             double r2 = dx * dx + dy * dy + dz * dz;
-            for (int ip = 0; ip < npi; ip++)
-                for (int jp = 0; jp < npj; jp++, off++) {
+            // primitive pairs whose Gaussian-product factor exp(-ai aj/(ai+aj) r^2)
+            // is above exp(-JK_PRIM_EXPCUT) first, their count in h_pnp
+            // (the thread kernels loop over those only; the others carry a
+            // factor below 1e-26 and are kept after them for the kernels
+            // that loop over all)
+            std::vector<std::pair<int, int>> order;
+            for (int pass = 0; pass < 2; pass++)
+                for (int ip = 0; ip < npi; ip++)
+                    for (int jp = 0; jp < npj; jp++) {
+                        const bool kept = r2 * ai[ip] * aj[jp] / (ai[ip] + aj[jp]) <= JK_PRIM_EXPCUT;
+                        if (kept == (pass == 0)) order.push_back({ip, jp});
+                        if (pass == 0 && kept) b->h_pnp[p]++;
+                    }
+            for (const auto& pr : order) {
+                const int ip = pr.first, jp = pr.second;
+                {
                     double aij = ai[ip] + aj[jp];
                     a12[off] = aij;
                     ia12[off] = 1. / aij;
@@ -625,8 +645,11 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
                     primf[4 * npp + off] = (float)(aj[jp] * (rj[1] - ri[1]) / aij);
                     primf[5 * npp + off] = (float)(aj[jp] * (rj[2] - ri[2]) / aij);
                 }
+                off++;
+            }
         }
     }
+    CUDA_TRY(upload(&b->d_pnp, b->h_pnp.data(), b->h_pnp.size()));
     CUDA_TRY(upload(&b->d_prim, prim.data(), prim.size()));
     CUDA_TRY(upload(&b->d_primf, primf.data(), primf.size()));
     {
@@ -782,6 +805,7 @@ static void fill_seg(const jk_basis* b, int cp_ij, int cp_kl, const long long* q
     s->npf = n;
     s->bas_x = b->d_bas_x;
     s->pgeo = b->d_pgeo;
+    s->pnp = b->d_pnp;
     s->pao = b->d_pao;
     s->npt = (int)b->h_pair2bra.size();
     s->nbas = b->nbas;

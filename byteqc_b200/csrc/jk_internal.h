@@ -135,6 +135,8 @@ struct jk_basis {
     size_t h_qoff1_cap = 0;
     JKFanout fan;  // side streams of the class launches
     double* d_pgeo = nullptr;  // pair geometry (JKSeg::pgeo)
+    std::vector<int> h_pnp;    // primitive pairs above the exponent cutoff, per pair
+    int* d_pnp = nullptr;
     int* d_pao = nullptr;      // first AOs of the pair's shells (JKSeg::pao)
     // pair-packed J side of jk_build
     std::vector<JKPackCls> h_pack;

@@ -511,7 +511,8 @@ __device__ __forceinline__ void jk_thread_pass(const JKSeg& sg, const JKQuartet&
             ac[d] = (float)(ri[d] - rk[d]);
         }
         const float normf = (float)q.norm;
-        const int npij = sg.nprim_ij, npkl = sg.nprim_kl;
+        const int npij = sg.pnp ? __ldg(sg.pnp + q.bij) : sg.nprim_ij;
+        const int npkl = sg.pnp ? __ldg(sg.pnp + q.bkl) : sg.nprim_kl;
         JKPPF kn = jk_ppf(sg, q.prim_kl);
         for (int kp = 0; kp < npkl; kp++) {
             const JKPPF kc = kn;
@@ -531,7 +532,8 @@ __device__ __forceinline__ void jk_thread_pass(const JKSeg& sg, const JKQuartet&
             }
         }
     } else {
-        const int npij = sg.nprim_ij, npkl = sg.nprim_kl;
+        const int npij = sg.pnp ? __ldg(sg.pnp + q.bij) : sg.nprim_ij;
+        const int npkl = sg.pnp ? __ldg(sg.pnp + q.bkl) : sg.nprim_kl;
         JKPP kn = jk_pp(sg, q.prim_kl);
         for (int kp = 0; kp < npkl; kp++) {
             const JKPP kc = kn;
