@@ -35,6 +35,7 @@ WORKLOADS = {
     'h2o32-tzvp': (32, 14.0, 2, 'standin-def2-tzvp'),
     'h2o8-dz': (8, 9.0, 0, 'standin-cc-pvdz'),
     'h2o64-dz': (64, 18.0, 3, 'standin-cc-pvdz'),
+    'h2o12-tzvp': (12, 10.5, 2, 'standin-def2-tzvp'),  # small case for ncu captures
 }
 
 
@@ -357,6 +358,31 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def profile_builds(args, torch, lib):
+    """jk_build of the workload density in the working basis, repeated (for
+    ncu launch lists and captures); prints nothing but a line count."""
+    import ctypes
+    from byteqc_b200.cuobc import lib as jklib
+    from byteqc_b200.cuobc.scf import hf
+    mol, dm = make_workload(args.workload)
+    opt = hf._VHFOpt(mol).build()
+    nao = opt.coeff.shape[0]
+    C = opt.coeff_dev
+    w = (C @ torch.as_tensor(dm, device='cuda') @ C.T).contiguous()
+    vj = torch.zeros(nao, nao, dtype=torch.float64, device='cuda')
+    vk = torch.zeros_like(vj)
+    o = jklib.JKOpts()
+    o.direct_scf_tol = opt.direct_scf_tol
+    o.nbins = opt.default_nbins()
+    o.prescreen = 1
+    o.fp32_cutoff = args.fp32_cutoff if '--fp32-cutoff' in sys.argv else 0.
+    for _ in range(args.profile_builds):
+        jklib.check(lib.jk_build(opt.handle, w.data_ptr(), 1, vj.data_ptr(),
+                                 vk.data_ptr(), ctypes.byref(o), None), 'jk_build')
+    torch.cuda.synchronize()
+    print('profile builds done: %d x %s' % (args.profile_builds, args.workload))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -365,6 +391,10 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--workload', default='h2o32-tzvp', choices=sorted(WORKLOADS))
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--profile-builds', type=int, default=0,
+                    help='only run this many jk_build calls of the workload '
+                         '(FP64, or mixed with --fp32-cutoff > 0 given '
+                         'explicitly) and exit: the command profiled by ncu')
     ap.add_argument('--ref-sample-s', type=float, default=8.0)
     ap.add_argument('--batch-mols', type=int, default=256,
                     help='molecules of the batched workload (0: skip)')
@@ -402,6 +432,8 @@ def main():
         dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=300))
 
     lib = jklib.load_library()
+    if args.profile_builds > 0:
+        return profile_builds(args, torch, lib)
     mol, dm = make_workload(args.workload)
     t = time.perf_counter()
     opt = hf._VHFOpt(mol).build()
