@@ -293,6 +293,40 @@ __device__ __forceinline__ void rys_roots_all_f(const float* __restrict__ tab, f
     }
 }
 
+// root r only (runtime r), single precision, from the float table copy
+template <int N>
+__device__ __forceinline__ void rys_root_one_f(const float* __restrict__ tab, float x, int r, float& s, float& w) {
+    using S = RysS<N>;
+    if (N == 1) {
+        float f0, f1;
+        boys01_f(x, f0, f1);
+        w = f0;
+        s = __fdividef(f1, f0);
+        return;
+    }
+    if (x >= (float)S::XMAX) {
+        const float srx = rsqrtf(x);
+        s = tab[S::HERM + r] * srx * srx;
+        w = tab[S::HERM + N + r] * srx;
+        return;
+    }
+    const int m = (int)(x * 0.5f);
+    const float t = x - (float)(2 * m + 1), t2 = t + t;
+    const float* c = tab + m * S::STRIDE;
+    float bs1 = 0.f, bs2 = 0.f, bw1 = 0.f, bw2 = 0.f;
+#pragma unroll
+    for (int k = RYS_NC - 1; k >= 1; k--) {
+        float b0 = fmaf(t2, bs1, c[k * S::NS + r] - bs2);
+        bs2 = bs1;
+        bs1 = b0;
+        b0 = fmaf(t2, bw1, c[k * S::NS + N + r] - bw2);
+        bw2 = bw1;
+        bw1 = b0;
+    }
+    s = fmaf(t, bs1, c[r] - bs2);
+    w = fmaf(t, bw1, c[N + r] - bw2);
+}
+
 // ---------------------------------------------------------------------------
 // Compile-time class description for (li lj | lk ll), li >= lj, lk >= ll.
 // ---------------------------------------------------------------------------

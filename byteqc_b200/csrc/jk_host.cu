@@ -1101,11 +1101,12 @@ extern "C" int jk_fma_peak(int fp32, double* tflops) {
 // paths the kernels use: mode 0 all roots from the shared-memory copy (thread
 // kernels), 1 one root at a time from it (team kernels), 2 one root from the
 // global table (setup kernels), 3 all roots in single precision (the FP32
-// quartets of the mixed mode, n <= JK_F32_ROOTS)
+// quartets of the mixed mode, n <= JK_F32_ROOTS; thread kernels), 4 one root
+// at a time in single precision (team kernels)
 template <int N>
 __global__ void jk_rys_eval_kernel(const double* rys, const double* x, int count, double* s, double* w, int mode) {
     extern __shared__ __align__(16) double tab[];
-    if (mode == 3) rys_table_to_smem_f<N>(rys, reinterpret_cast<float*>(tab));
+    if (mode >= 3) rys_table_to_smem_f<N>(rys, reinterpret_cast<float*>(tab));
     else rys_table_to_smem<N>(rys, tab);
     __syncthreads();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1117,6 +1118,15 @@ __global__ void jk_rys_eval_kernel(const double* rys, const double* x, int count
             for (int r = 0; r < N; r++) {
                 s[i * N + r] = rs[r];
                 w[i * N + r] = rw[r];
+            }
+        }
+    } else if (mode == 4) {
+        if constexpr (N <= JK_F32_ROOTS) {
+            for (int r = 0; r < N; r++) {
+                float rs, rw;
+                rys_root_one_f<N>(reinterpret_cast<const float*>(tab), (float)x[i], r, rs, rw);
+                s[i * N + r] = rs;
+                w[i * N + r] = rw;
             }
         }
     } else if (mode == 0) {
@@ -1145,8 +1155,8 @@ static cudaError_t rys_eval_launch(const double* rys, const double* x, int count
 }
 
 extern "C" int jk_rys_roots_device(int n, const double* x, int count, double* s, double* w, int mode, void* stream) {
-    if (n < 1 || n > 11 || !x || !s || !w || count < 0 || mode < 0 || mode > 3 ||
-        (mode == 3 && n > JK_F32_ROOTS))
+    if (n < 1 || n > 11 || !x || !s || !w || count < 0 || mode < 0 || mode > 4 ||
+        (mode >= 3 && n > JK_F32_ROOTS))
         return set_err(JK_ERR_ARG, "jk_rys_roots_device: bad args");
     if (count == 0) return JK_OK;
     const double* rys;

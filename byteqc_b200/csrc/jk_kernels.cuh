@@ -692,7 +692,13 @@ __device__ __forceinline__ void jk_team_body(const Src& src) {
     double* part = reinterpret_cast<double*>(g);  // digestion partials reuse the 2D-block space
     double* buf = reinterpret_cast<double*>(gbase + jk_team_gbytes<C, R>()) + (size_t)team * S::BWORDS;
     const JKSeg& sg0 = src.first();
-    if (S::SMEM_TAB) rys_table_to_smem<NR>(sg0.rys, tab);
+    // FP32 quartets at low order: float prefactors, nodes and weights (the
+    // table copy in shared memory is then single precision)
+    constexpr bool F32P = JKF32Prim<C, R>::value && S::SMEM_TAB;
+    if (S::SMEM_TAB) {
+        if constexpr (F32P) rys_table_to_smem_f<NR>(sg0.rys, reinterpret_cast<float*>(tab));
+        else rys_table_to_smem<NR>(sg0.rys, tab);
+    }
 
     // owned Cartesian indices
     int ci = 0, cj = 0;
@@ -738,18 +744,42 @@ __device__ __forceinline__ void jk_team_body(const Src& src) {
         R acc[C::NACC];
 #pragma unroll
         for (int e = 0; e < C::NACC; e++) acc[e] = R(0);
+        float dijf[3], dklf[3], acf[3];
+        if (F32P && active) {
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                dijf[d] = (float)(ri[d] - rj[d]);
+                dklf[d] = (float)(rk[d] - rl[d]);
+                acf[d] = (float)(ri[d] - rk[d]);
+            }
+        }
         for (int kp = 0; kp < nprim_kl; kp++) {
             JKPP kc;
-            if (active) kc = jk_pp(sg, q.prim_kl + kp);
+            JKPPF kcf;
+            if (active) {
+                if constexpr (F32P) kcf = jk_ppf(sg, q.prim_kl + kp);
+                else kc = jk_pp(sg, q.prim_kl + kp);
+            }
             for (int ip = 0; ip < nprim_ij; ip++) {
                 if (active) {
-                    JKPrim p = jk_prim2(jk_pp(sg, q.prim_ij + ip), kc);
-                    for (int u = lane; u < 3 * NR; u += T) {
-                        int r = u / 3, d = u - 3 * r;
-                        double s, w;
-                        if (S::SMEM_TAB) rys_root_one<NR>(tab, p.x, r, s, w);
-                        else rys_root<NR>(sg.rys, p.x, r, s, w);
-                        jk_unit<C, R>(p, s, w, d, q.norm, ri, rj, rk, rl, g + u * C::GS);
+                    if constexpr (F32P) {
+                        const JKPrimF pf = jk_prim_f2(jk_ppf(sg, q.prim_ij + ip), kcf, acf);
+                        const float normf = (float)q.norm;
+                        for (int u = lane; u < 3 * NR; u += T) {
+                            int r = u / 3, d = u - 3 * r;
+                            float s, w;
+                            rys_root_one_f<NR>(reinterpret_cast<const float*>(tab), pf.x, r, s, w);
+                            jk_unit_f<C>(pf, s, w, d, normf, dijf, dklf, g + u * C::GS);
+                        }
+                    } else {
+                        JKPrim p = jk_prim2(jk_pp(sg, q.prim_ij + ip), kc);
+                        for (int u = lane; u < 3 * NR; u += T) {
+                            int r = u / 3, d = u - 3 * r;
+                            double s, w;
+                            if (S::SMEM_TAB) rys_root_one<NR>(tab, p.x, r, s, w);
+                            else rys_root<NR>(sg.rys, p.x, r, s, w);
+                            jk_unit<C, R>(p, s, w, d, q.norm, ri, rj, rk, rl, g + u * C::GS);
+                        }
                     }
                 }
                 __syncthreads();

@@ -147,7 +147,8 @@ int jk_rys_roots_host(int n, double x, double *s, double *w);
 /* The same tables evaluated by a device kernel through the paths the J/K
  * kernels use (mode 0: all roots from the shared-memory copy, 1: one root at
  * a time from it, 2: one root from the global copy, 3: all roots in single
- * precision as the FP32 quartets of the mixed mode use them, n <= 3 only;
+ * precision as the FP32 quartets of the mixed mode use them, 4: one root at a
+ * time in single precision; modes 3 and 4 for n <= 3 only;
  * n = 1 is evaluated from the Boys function in every mode).  x, s, w are device arrays (count,
  * count*n, count*n).  For checking the device evaluation. */
 int jk_rys_roots_device(int n, const double *x, int count, double *s, double *w, int mode, void *stream);

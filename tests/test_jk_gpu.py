@@ -121,17 +121,19 @@ def test_device_rys_fp32_nodes():
                          rng.uniform(0, 60, 300)])
     dx = torch.as_tensor(xs, device='cuda')
     for n in range(1, 4):
-        ds = torch.zeros(len(xs) * n, dtype=torch.float64, device='cuda')
-        dw = torch.zeros_like(ds)
-        assert lib.jk_rys_roots_device(n, dx.data_ptr(), len(xs), ds.data_ptr(),
-                                       dw.data_ptr(), 3, None) == 0
-        s = ds.cpu().numpy().reshape(-1, n)
-        w = dw.cpu().numpy().reshape(-1, n)
-        for i, x in enumerate(xs):
-            hs, hw = np.zeros(n), np.zeros(n)
-            lib.jk_rys_roots_host(n, x, hs.ctypes.data, hw.ctypes.data)
-            assert abs(s[i] - hs).max() <= 2e-6, (n, x, s[i], hs)
-            assert abs(w[i] - hw).max() <= 2e-6 * hw.sum(), (n, x, w[i], hw)
+        for mode in (3, 4):  # all roots at once (thread kernels), one at a time (teams)
+            ds = torch.zeros(len(xs) * n, dtype=torch.float64, device='cuda')
+            dw = torch.zeros_like(ds)
+            assert lib.jk_rys_roots_device(n, dx.data_ptr(), len(xs),
+                                           ds.data_ptr(), dw.data_ptr(), mode,
+                                           None) == 0
+            s = ds.cpu().numpy().reshape(-1, n)
+            w = dw.cpu().numpy().reshape(-1, n)
+            for i, x in enumerate(xs):
+                hs, hw = np.zeros(n), np.zeros(n)
+                lib.jk_rys_roots_host(n, x, hs.ctypes.data, hw.ctypes.data)
+                assert abs(s[i] - hs).max() <= 2e-6, (n, mode, x, s[i], hs)
+                assert abs(w[i] - hw).max() <= 2e-6 * hw.sum(), (n, mode, x, w[i], hw)
     # higher orders are not evaluated in single precision
     assert lib.jk_rys_roots_device(4, dx.data_ptr(), 1, ds.data_ptr(),
                                    dw.data_ptr(), 3, None) != 0
