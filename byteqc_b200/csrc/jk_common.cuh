@@ -11,7 +11,22 @@
 #define RYS_META static __constant__
 #include "rys_table.h"
 
-#define JK_LMAX 3  // angular momentum handled by the templated kernels
+#define JK_LMAX 3      // angular momentum handled by the templated kernels
+#define JK_LMAX_ALL 5  // ... and by the generic kernel (jk_generic.cu): up to h
+// launcher tables are indexed by the class (li lj | lk ll), base 6
+#define JK_CLASS_INDEX(li, lj, lk, ll) ((((li) * 6 + (lj)) * 6 + (lk)) * 6 + (ll))
+#define JK_NCLASS 1296
+
+// libcint slots (cuobc/lib/gint/gint.h:29-46)
+#define ATM_SLOTS 6
+#define PTR_COORD 1
+#define BAS_SLOTS 8
+#define ATOM_OF 0
+#define ANG_OF 1
+#define NPRIM_OF 2
+#define NCTR_OF 3
+#define PTR_EXP 5
+#define PTR_COEFF 6
 
 // 2 pi^3 / sqrt(pi): prefactor of the two-electron integrals (the seed of the
 // x 2D integrals; cuobc/lib/gint/g2e.c:41)
@@ -491,6 +506,7 @@ struct JKSeg {
     double* jp_kl;
     int np_ij, np_kl;        // pairs of each class (component stride)
     long long pk_stride;     // packed elements per density
+    int ls[4];               // angular momenta of the class (read by the generic kernel)
 };
 
 // launchers of one class: a single segment (by value) or a segment table

@@ -54,19 +54,10 @@ static std::once_flag g_tab_once;
 static void init_tables() {
     std::call_once(g_tab_once, [] {
         JK_REGISTER_ALL();
+        jk_register_generic(&g_tabs);
     });
 }
 
-// libcint slots (cuobc/lib/gint/gint.h:29-46)
-#define ATM_SLOTS 6
-#define PTR_COORD 1
-#define BAS_SLOTS 8
-#define ATOM_OF 0
-#define ANG_OF 1
-#define NPRIM_OF 2
-#define NCTR_OF 3
-#define PTR_EXP 5
-#define PTR_COEFF 6
 
 static double common_fac_sp(int l) {
     return l == 0 ? 0.282094791773878143 : (l == 1 ? 0.488602511902919921 : 1.0);
@@ -152,6 +143,10 @@ __global__ void jk_qcond_kernel(const int* __restrict__ pi, const int* __restric
     q[(size_t)ish * nbas + jsh] = v;
     q[(size_t)jsh * nbas + ish] = v;
 }
+
+// Schwarz diagonal of pairs with a shell above f (jk_generic.cu)
+void jk_qcond_generic(const int* pi, const int* pj, int n, const int* atm, const int* bas, const double* env,
+                      int nbas, double* q, const double* rys, cudaStream_t st);
 
 typedef void (*qcond_fn)(const int*, const int*, int, const int*, const int*, const double*, int, double*,
                          const double*, cudaStream_t);
@@ -485,8 +480,8 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
     b->h_ao_loc[0] = 0;
     for (int i = 0; i < nbas; i++) {
         int l = bas[i * BAS_SLOTS + ANG_OF];
-        if (l < 0 || l > JK_LMAX)
-            return set_err(JK_ERR_UNSUPPORTED, "shell %d has l=%d; this engine handles l <= %d", i, l, JK_LMAX);
+        if (l < 0 || l > JK_LMAX_ALL)
+            return set_err(JK_ERR_UNSUPPORTED, "shell %d has l=%d; this engine handles l <= %d", i, l, JK_LMAX_ALL);
         if (bas[i * BAS_SLOTS + NCTR_OF] != 1)
             return set_err(JK_ERR_ARG, "shell %d: generally contracted shells must be split first", i);
         b->h_ao_loc[i + 1] = b->h_ao_loc[i] + (l + 1) * (l + 2) / 2;
@@ -524,21 +519,24 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
     CUDA_TRY(cudaMalloc(&b->d_qcond, sizeof(double) * (size_t)nbas * nbas));
     CUDA_TRY(cudaMemset(b->d_qcond, 0, sizeof(double) * (size_t)nbas * nbas));
     {
-        std::vector<int> pi[4][4], pj[4][4];
+        std::vector<int> pi[JK_LMAX_ALL + 1][JK_LMAX_ALL + 1], pj[JK_LMAX_ALL + 1][JK_LMAX_ALL + 1];
         for (int i = 0; i < nbas; i++)
             for (int j = 0; j <= i; j++) {
                 int li = bas[i * BAS_SLOTS + ANG_OF], lj = bas[j * BAS_SLOTS + ANG_OF];
                 if (li >= lj) { pi[li][lj].push_back(i); pj[li][lj].push_back(j); }
                 else { pi[lj][li].push_back(j); pj[lj][li].push_back(i); }
             }
-        for (int a = 0; a < 4; a++)
+        for (int a = 0; a <= JK_LMAX_ALL; a++)
             for (int c = 0; c <= a; c++) {
                 int n = (int)pi[a][c].size();
                 if (!n) continue;
                 int *dpi, *dpj;
                 CUDA_TRY(upload(&dpi, pi[a][c].data(), n));
                 CUDA_TRY(upload(&dpj, pj[a][c].data(), n));
-                g_qcond[a][c](dpi, dpj, n, b->d_atm, b->d_bas, b->d_env, nbas, b->d_qcond, b->rys, 0);
+                if (a <= JK_LMAX)
+                    g_qcond[a][c](dpi, dpj, n, b->d_atm, b->d_bas, b->d_env, nbas, b->d_qcond, b->rys, 0);
+                else
+                    jk_qcond_generic(dpi, dpj, n, b->d_atm, b->d_bas, b->d_env, nbas, b->d_qcond, b->rys, 0);
                 cudaError_t e = cudaGetLastError();
                 if (e == cudaSuccess) e = cudaDeviceSynchronize();
                 cudaFree(dpi);
@@ -817,13 +815,17 @@ static void fill_seg(const jk_basis* b, int cp_ij, int cp_kl, const long long* q
     s->jp_ij = s->jp_kl = nullptr;
     s->np_ij = s->np_kl = 0;
     s->pk_stride = 0;
+    s->ls[0] = b->h_group_l[b->h_cls_gi[cp_ij]];
+    s->ls[1] = b->h_group_l[b->h_cls_gj[cp_ij]];
+    s->ls[2] = b->h_group_l[b->h_cls_gi[cp_kl]];
+    s->ls[3] = b->h_group_l[b->h_cls_gj[cp_kl]];
 }
 
 int jk_internal_class_index(const jk_basis_t* b, int cp_ij, int cp_kl);
 static int class_index(const jk_basis* b, int cp_ij, int cp_kl) {
     int li = b->h_group_l[b->h_cls_gi[cp_ij]], lj = b->h_group_l[b->h_cls_gj[cp_ij]];
     int lk = b->h_group_l[b->h_cls_gi[cp_kl]], ll = b->h_group_l[b->h_cls_gj[cp_kl]];
-    return li * 64 + lj * 16 + lk * 4 + ll;
+    return JK_CLASS_INDEX(li, lj, lk, ll);
 }
 
 extern "C" int jk_build(jk_basis_t* b, const double* dm, int n_dm, double* vj, double* vk, const jk_opts_t* opts,

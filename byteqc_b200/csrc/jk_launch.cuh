@@ -1,5 +1,5 @@
 // Launchers of the J/K kernels, one per (li, lj, lk, ll) class and arithmetic
-// type, collected in a table indexed by li*64 + lj*16 + lk*4 + ll.
+// type, collected in a table indexed by JK_CLASS_INDEX(li, lj, lk, ll).
 #pragma once
 #include "jk_kernels.cuh"
 
@@ -80,23 +80,26 @@ cudaError_t jk_launch_batch(const JKSeg* segs, const long long* segt, int nseg, 
     return cudaGetLastError();
 }
 
-// launcher tables indexed by li*64 + lj*16 + lk*4 + ll
+// launcher tables indexed by JK_CLASS_INDEX(li, lj, lk, ll)
 struct JKTables {
-    jk_launch_fn t64[256], t32[256];
-    jk_launch_batch_fn b64[256], b32[256];
+    jk_launch_fn t64[JK_NCLASS], t32[JK_NCLASS];
+    jk_launch_batch_fn b64[JK_NCLASS], b32[JK_NCLASS];
 };
+
+// classes with a shell above f: the generic kernel (jk_generic.cu)
+void jk_register_generic(JKTables* T);
 
 // per-instantiation-file registration (jk_inst_*.cu, generated list)
 #include "jk_inst_list.h"
 
 #ifndef JK_NO_FP32
 #define JK_REG32(LI, LJ, LK, LL)                                         \
-    T->t32[(LI)*64 + (LJ)*16 + (LK)*4 + (LL)] = jk_launch<LI, LJ, LK, LL, float>; \
-    T->b32[(LI)*64 + (LJ)*16 + (LK)*4 + (LL)] = jk_launch_batch<LI, LJ, LK, LL, float>;
+    T->t32[JK_CLASS_INDEX(LI, LJ, LK, LL)] = jk_launch<LI, LJ, LK, LL, float>; \
+    T->b32[JK_CLASS_INDEX(LI, LJ, LK, LL)] = jk_launch_batch<LI, LJ, LK, LL, float>;
 #else
 #define JK_REG32(LI, LJ, LK, LL)
 #endif
 #define JK_REG(LI, LJ, LK, LL)                                                       \
-    T->t64[(LI)*64 + (LJ)*16 + (LK)*4 + (LL)] = jk_launch<LI, LJ, LK, LL, double>;  \
-    T->b64[(LI)*64 + (LJ)*16 + (LK)*4 + (LL)] = jk_launch_batch<LI, LJ, LK, LL, double>; \
+    T->t64[JK_CLASS_INDEX(LI, LJ, LK, LL)] = jk_launch<LI, LJ, LK, LL, double>;  \
+    T->b64[JK_CLASS_INDEX(LI, LJ, LK, LL)] = jk_launch_batch<LI, LJ, LK, LL, double>; \
     JK_REG32(LI, LJ, LK, LL)

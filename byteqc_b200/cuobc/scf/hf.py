@@ -23,7 +23,7 @@ import numpy as np
 from byteqc_b200.cuobc import lib as _lib
 from byteqc_b200.gto import mole as gmole
 
-LMAX_ON_GPU = 3  # f functions; the reference's GPU kernels go up to h
+LMAX_ON_GPU = 5  # h functions, as the reference's GPU kernels
 ANGULAR = 'spdfghik'
 
 

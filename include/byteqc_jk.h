@@ -10,7 +10,8 @@
  *
  * Working basis: the decontracted Cartesian basis with shells sorted into
  * groups of equal (l, nprim), exactly as the reference's _VHFOpt.build
- * prepares it (cuobc/scf/hf.py:288-330, 481-564).  Angular momentum up to f.
+ * prepares it (cuobc/scf/hf.py:288-330, 481-564).  Angular momentum up to h
+ * (l = 5), as the reference's GPU kernels.
  */
 #ifndef BYTEQC_JK_H
 #define BYTEQC_JK_H

@@ -78,3 +78,25 @@ def test_batch_identical_molecules_keep_their_own_j():
             scale = max(1.0, abs(vj).max())
             assert abs(res[m][0] - vj).max() <= 1e-10 * scale, (cut, m)
             assert abs(res[m][1] - vk).max() <= 1e-10 * scale, (cut, m)
+
+
+def test_batch_g_h_shells():
+    """Batched builds of molecules with g and h shells (the generic kernel's
+    segment-table launch) match the single-molecule builds."""
+    from byteqc_b200.cuobc.scf import hf
+    from byteqc_b200.cuobc.scf.batch import JKBatch
+    from byteqc_b200.gto import basis as basis_mod
+    extra = {'O': [[4, [1.1, 1.0]], [5, [0.9, 1.0]]], 'H': [[4, [0.8, 1.0]]]}
+    bas = {s: list(basis_mod.load('standin-cc-pvdz', s)) + extra[s]
+           for s in ('O', 'H')}
+    mols = [Mole(atom=geom.water_cluster(n, box=5.0, seed=s), basis=bas).build()
+            for n, s in ((1, 1), (2, 2), (1, 3))]
+    dms = _dms(mols, seed=5)
+    batch = JKBatch(mols)
+    for cut in (0., 1e-6):
+        res = batch.get_jk(dms, fp32_cutoff=cut)
+        for m, (mol, dm, opt) in enumerate(zip(mols, dms, batch.opts)):
+            vj, vk = hf.get_jk(mol, dm, vhfopt=opt, fp32_cutoff=cut)
+            scale = max(1.0, abs(vj).max())
+            assert abs(res[m][0] - vj).max() <= 1e-10 * scale
+            assert abs(res[m][1] - vk).max() <= 1e-10 * scale

@@ -215,3 +215,41 @@ def test_get_jk_vs_golden(case):
     vj, vk = hf.get_jk(mol, dm)
     _close(vj, g[case + '/vj'])
     _close(vk, g[case + '/vk'])
+
+
+def _high_l_mol(nw, seed=1):
+    """Water molecules in the cc-pVDZ stand-in plus g and h shells (an
+    uncontracted g and h and a two-primitive g on O, a g on H): every class
+    above f runs the generic kernel, next to the templated ones."""
+    from byteqc_b200.gto import basis as basis_mod
+    extra = {'O': [[4, [1.1, 1.0]], [5, [0.9, 1.0]], [4, [3.0, 0.6], [0.7, 0.5]]],
+             'H': [[4, [0.8, 1.0]]]}
+    bas = {s: list(basis_mod.load('standin-cc-pvdz', s)) + extra[s]
+           for s in ('O', 'H')}
+    return Mole(atom=geom.water_cluster(nw, box=5.0, seed=seed),
+                basis=bas).build()
+
+
+@pytest.mark.parametrize('nw', [1, 2])
+def test_get_jk_g_h_shells_vs_oracle(nw):
+    from byteqc_b200.cuobc.scf import hf
+    from oracle import hf_oracle
+    mol = _high_l_mol(nw)
+    assert int(mol._bas[:, 1].max()) == 5
+    opt = hf._VHFOpt(mol).build()
+    ropt = hf_oracle.VHFOpt(mol).build()
+    np.testing.assert_allclose(opt.q_cond, ropt.q_cond, rtol=1e-11,
+                               atol=1e-16)
+    dm = _rand_dm(mol.nao, ndm=2)
+    rj, rk = hf_oracle.get_jk(mol, dm, vhfopt=ropt)
+    vj, vk = hf.get_jk(mol, dm, vhfopt=opt)
+    _close(vj, rj)
+    _close(vk, rk)
+    # the reference's class-pair task loop reaches the same kernels
+    cj, ck = hf.get_jk_class_pairs(mol, dm, opt)
+    _close(cj.cpu().numpy(), rj)
+    _close(ck.cpu().numpy(), rk)
+    # mixed mode: the generic classes stay in FP64 in both parts
+    mj, mk = hf.get_jk(mol, dm, vhfopt=opt, fp32_cutoff=1e-6)
+    scale = max(1.0, abs(vj).max())
+    assert max(abs(mj - vj).max(), abs(mk - vk).max()) < 1e-4 * scale

@@ -74,6 +74,33 @@ def test_eri_vs_obara_saika():
         assert abs(a - b).max() <= 1e-12 * abs(b).max() + 1e-14, lq
 
 
+def test_eri_vs_obara_saika_g_h():
+    """Quartets with g and h shells (the classes of the generic GPU kernel):
+    the oracle's Rys engine against Obara-Saika."""
+    import oracle
+    from oracle import eri_os
+    from oracle import hf_oracle
+    from byteqc_b200.gto import basis as basis_mod
+    extra = {'O': [[4, [1.1, 1.0]], [5, [0.9, 1.0]],
+                   [4, [3.0, 0.6], [0.7, 0.5]]],
+             'H': [[4, [0.8, 1.0]]]}
+    bas = {s: list(basis_mod.load('standin-cc-pvdz', s)) + extra[s]
+           for s in ('O', 'H')}
+    mol = Mole(atom=geom.water_cluster(1, box=4.0, seed=2), basis=bas).build()
+    pm = hf_oracle.VHFOpt(mol).build().mol
+    rng = np.random.default_rng(0)
+    ls = pm._bas[:, 1]
+    by_l = {l: np.flatnonzero(ls == l) for l in (0, 1, 2, 4, 5)}
+    picks = [(4, 0, 0, 0), (5, 1, 2, 0), (4, 4, 1, 0), (5, 4, 2, 2),
+             (5, 5, 1, 1)]
+    for lq in picks:
+        sh = [int(rng.choice(by_l[l])) for l in lq]
+        a = oracle.eri_shells(pm, *sh)
+        b = eri_os.eri_shells(pm, *sh)
+        assert a.shape == b.shape
+        assert abs(a - b).max() <= 1e-12 * abs(b).max() + 1e-14, lq
+
+
 def test_jk_vs_full_eri_tensor():
     """Oracle get_jk (screened, binned, 8-fold symmetric loop) against J and K
     contracted from the full ERI tensor of the working basis."""
