@@ -396,9 +396,10 @@ struct JKClass {
 // then the horizontal transfers (a, j+1) = (a+1, j) + (Ri - Rj)(a, j) and
 // (c, l+1) = (c+1, l) + (Rk - Rl)(c, l).  Same recursion as the reference's
 // GINTg0_2e_2d4d (cuobc/lib/gvhf/g2e.cu:66-166), written here as explicit
-// register arrays.  Output: I[((i*(LJ+1)+j)*(LK+1)+k)*(LL+1)+l].
+// register arrays.  Output: I[i*XSI + j*XSJ + k*(LL+1) + l], by default the
+// packed layout I[((i*(LJ+1)+j)*(LK+1)+k)*(LL+1)+l].
 // ---------------------------------------------------------------------------
-template <typename R, class C, typename OutT>
+template <typename R, class C, int XSI = C::SI, int XSJ = C::SJ, typename OutT>
 __device__ __forceinline__ void rys_2d(R seed, R c00, R c0p, R b10, R b01, R b00, R dij, R dkl,
                                        OutT* __restrict__ I) {
     constexpr int NM = C::NM, MM = C::MM;
@@ -442,13 +443,13 @@ __device__ __forceinline__ void rys_2d(R seed, R c00, R c0p, R b10, R b01, R b00
 #pragma unroll
             for (int c = 0; c <= MM; c++) B[c] = H[i][j][c];
 #pragma unroll
-            for (int k = 0; k <= C::LK; k++) I[i * C::SI + j * C::SJ + k * C::SK] = B[k];
+            for (int k = 0; k <= C::LK; k++) I[i * XSI + j * XSJ + k * C::SK] = B[k];
 #pragma unroll
             for (int l = 1; l <= C::LL; l++) {
 #pragma unroll
                 for (int c = 0; c + l <= MM; c++) B[c] = B[c + 1] + dkl * B[c];
 #pragma unroll
-                for (int k = 0; k <= C::LK; k++) I[i * C::SI + j * C::SJ + k * C::SK + l] = B[k];
+                for (int k = 0; k <= C::LK; k++) I[i * XSI + j * XSJ + k * C::SK + l] = B[k];
             }
         }
 }

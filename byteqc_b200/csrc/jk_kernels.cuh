@@ -190,8 +190,8 @@ __device__ __forceinline__ JKPrim jk_prim2(const JKPP& b, const JKPP& k) {
     return p;
 }
 
-// build the 2D block of (axis d, root r) into out
-template <class C, typename R, typename OutT>
+// build the 2D block of (axis d, root r) into out (strides XSI, XSJ of i, j)
+template <class C, typename R, int XSI = C::SI, int XSJ = C::SJ, typename OutT>
 __device__ __forceinline__ void jk_unit(const JKPrim& p, double s, double w, int d, double norm, const double* ri,
                                         const double* rj, const double* rk, const double* rl, OutT* out) {
     // select by d without dynamic indexing (keeps everything in registers)
@@ -207,7 +207,7 @@ __device__ __forceinline__ void jk_unit(const JKPrim& p, double s, double w, int
     double c00 = (Pd - Rid) - bs * pq;
     double c0p = (Qd - Rkd) + as * pq;
     double seed = d == 0 ? norm : (d == 1 ? p.sy : w);
-    rys_2d<R, C>((R)seed, (R)c00, (R)c0p, (R)b10, (R)b01, (R)b00, (R)(Rid - Rjd), (R)(Rkd - Rld), out);
+    rys_2d<R, C, XSI, XSJ>((R)seed, (R)c00, (R)c0p, (R)b10, (R)b01, (R)b00, (R)(Rid - Rjd), (R)(Rkd - Rld), out);
 }
 
 // ---------------------------------------------------------------------------
@@ -259,7 +259,7 @@ __device__ __forceinline__ JKPrimF jk_prim_f2(const JKPPF& b, const JKPPF& k, co
     return p;
 }
 
-template <class C, typename OutT>
+template <class C, int XSI = C::SI, int XSJ = C::SJ, typename OutT>
 __device__ __forceinline__ void jk_unit_f(const JKPrimF& p, float s, float w, int d, float norm, const float* dij,
                                           const float* dkl, OutT* out) {
     float siAB = s * p.iAB;
@@ -271,7 +271,7 @@ __device__ __forceinline__ void jk_unit_f(const JKPrimF& p, float s, float w, in
     float c00 = JK_PICK(p.PA) - bs * pq;
     float c0p = JK_PICK(p.QC) + as * pq;
     float seed = d == 0 ? norm : (d == 1 ? p.sy : w);
-    rys_2d<float, C>(seed, c00, c0p, b10, b01, b00, JK_PICK(dij), JK_PICK(dkl), out);
+    rys_2d<float, C, XSI, XSJ>(seed, c00, c0p, b10, b01, b00, JK_PICK(dij), JK_PICK(dkl), out);
 }
 #undef JK_PICK
 
@@ -639,8 +639,6 @@ template <class C>
 struct JKTeamShape {
     static constexpr int QPB = (C::T >= 128) ? 1 : (128 / C::T);  // quartets per block
     static constexpr int THREADS = QPB * C::T;
-    // per-team strides are odd so that teams start in different banks
-    static constexpr int GWORDS = (3 * C::NROOTS * C::GS) | 1;  // 2D blocks per quartet
     static constexpr int BWORDS_RAW = C::NFI * C::NFJ + C::NFK * C::NFL + C::NFI * C::NFK + C::NFI * C::NFL +
                                       C::NFJ * C::NFK + C::NFJ * C::NFL;  // digestion buffers
     static constexpr int BWORDS = BWORDS_RAW | 1;
@@ -658,14 +656,121 @@ struct JKTeamShape {
                          OFF_KJL = OFF_KJK + C::NFJ * C::NFK;
 };
 
+// ---------------------------------------------------------------------------
+// Shared-memory layout of a team's 2D blocks, padded against bank conflicts.
+// Two access patterns dominate: the products, where the thread owning bra
+// component ci (and cj) reads element own + o of every block with
+// own = lx(ci)*SI (+ lx(cj)*SJ) and o the same for the whole warp; and the
+// construction, where lane u writes element idx of unit u at u*GS + idx.  SI
+// (and SJ) are padded so that the owned offsets of a team fall in distinct
+// banks, GS is odd, and the team stride (the region of one team, which also
+// holds the digestion partials) is chosen modulo the bank count so that the
+// teams sharing a warp stay apart.  The choice is made at compile time with a
+// model of one warp access: the largest number of distinct addresses that
+// fall in one bank (bank = element index mod 128 / sizeof(R)).
+// ---------------------------------------------------------------------------
+constexpr int jk_bank_ways(const int* a, int n, int nb) {
+    int cnt[32] = {};
+    for (int i = 0; i < n; i++) {
+        bool dup = false;
+        for (int j = 0; j < i; j++)
+            if (a[j] == a[i]) {
+                dup = true;
+                break;
+            }
+        if (!dup) cnt[a[i] % nb]++;
+    }
+    int w = 0;
+    for (int b = 0; b < nb; b++) w = cnt[b] > w ? cnt[b] : w;
+    return w;
+}
+
+template <class C>
+constexpr int jk_team_own(int lane, int d, int si, int sj) {
+    const int ci = C::P == 1 ? lane : lane / C::NFJ;
+    const int cj = C::P == 1 ? 0 : lane - ci * C::NFJ;
+    const int ei = d == 0 ? cart_lx(C::LI, ci) : (d == 1 ? cart_ly(C::LI, ci) : cart_lz(C::LI, ci));
+    const int ej = C::P == 1 ? 0 : (d == 0 ? cart_lx(C::LJ, cj) : (d == 1 ? cart_ly(C::LJ, cj) : cart_lz(C::LJ, cj)));
+    return ei * si + ej * sj;
+}
+
+// distinct-bank spread of the owned offsets of one team (worst multiplicity)
+template <class C>
+constexpr int jk_team_own_ways(int si, int sj, int nb) {
+    int a[32] = {};
+    int n = 0;
+    for (int x = 0; x <= C::LI; x++)
+        for (int y = 0; y <= (C::P == 2 ? C::LJ : 0); y++) a[n++] = x * si + y * sj;
+    return jk_bank_ways(a, n, nb);
+}
+
+// bank ways summed over the warps of a block: three product reads (x, y, z
+// offsets) and one construction write per warp
+template <class C>
+constexpr int jk_team_ways(int si, int sj, int gs, int reg, int nb, int threads) {
+    int a[32] = {};
+    int total = 0;
+    for (int w = 0; w * 32 < threads; w++) {
+        const int t1 = threads < w * 32 + 32 ? threads : w * 32 + 32;
+        for (int d = 0; d < 3; d++) {
+            int n = 0;
+            for (int t = w * 32; t < t1; t++) a[n++] = (t / C::T) * reg + jk_team_own<C>(t % C::T, d, si, sj);
+            total += jk_bank_ways(a, n, nb);
+        }
+        int n = 0;
+        for (int t = w * 32; t < t1; t++)
+            if (t % C::T < 3 * C::NROOTS) a[n++] = (t / C::T) * reg + (t % C::T) * gs;
+        if (n) total += jk_bank_ways(a, n, nb);
+    }
+    return total;
+}
+
+template <class C>
+constexpr int jk_team_pick_si(int sj, int nb) {
+    const int s0 = C::P == 2 ? C::LJ * sj + C::SJ : C::SI;  // blocks of i do not overlap
+    int best = s0, bw = 1 << 20;
+    for (int s = s0; s < s0 + nb; s++) {
+        const int w = jk_team_own_ways<C>(s, sj, nb);
+        if (w < bw) {
+            bw = w;
+            best = s;
+        }
+    }
+    return best;
+}
+
+template <class C>
+constexpr int jk_team_pick_words(int si, int sj, int gs, int words0, int esize, int threads) {
+    int best = words0, bw = 1 << 20;
+    for (int r = 0; r < 16; r++) {
+        const int words = words0 + ((r - words0 % 16) + 16) % 16;
+        const int w = jk_team_ways<C>(si, sj, gs, words * 8 / esize, 128 / esize, threads);
+        if (w < bw) {
+            bw = w;
+            best = words;
+        }
+    }
+    return best;
+}
+
+template <class C, typename R>
+struct JKTeamLayout {
+    using S = JKTeamShape<C>;
+    static constexpr int NB = 128 / (int)sizeof(R);  // banks in elements of R
+    static constexpr int SJ = C::P == 2 ? (C::SJ | 1) : C::SJ;
+    static constexpr int SI = jk_team_pick_si<C>(SJ, NB);
+    static constexpr int GS = (C::LI * SI + C::LJ * SJ + (C::LK + 1) * (C::LL + 1)) | 1;  // elements per unit
+    // region of one team in doubles: the 2D blocks of all roots or the digestion partials
+    static constexpr int GW = (3 * C::NROOTS * GS * (int)sizeof(R) + 7) / 8;
+    static constexpr int WORDS0 = GW > S::PWORDS ? GW : S::PWORDS;
+    static constexpr int WORDS = jk_team_pick_words<C>(SI, SJ, GS, WORDS0, (int)sizeof(R), S::THREADS);
+};
+
 // bytes per team of the region shared by the 2D blocks and the digestion
-// partials (an odd number of doubles)
+// partials
 template <class C, typename R>
 __host__ __device__ constexpr size_t jk_team_region() {
-    using S = JKTeamShape<C>;
-    size_t g = (size_t)S::GWORDS * sizeof(R), p = (size_t)S::PWORDS * sizeof(double);
-    size_t words = ((g > p ? g : p) + 7) / 8;
-    return (words | 1) * 8;
+    return (size_t)JKTeamLayout<C, R>::WORDS * 8;
 }
 
 template <class C, typename R>
@@ -683,6 +788,7 @@ __host__ __device__ constexpr size_t jk_team_smem() {
 template <class C, typename R, class Src>
 __device__ __forceinline__ void jk_team_body(const Src& src) {
     using S = JKTeamShape<C>;
+    using L = JKTeamLayout<C, R>;
     constexpr int T = C::T, NR = C::NROOTS;
     extern __shared__ __align__(16) unsigned char jk_smem[];
     const int team = threadIdx.x / T, lane = threadIdx.x - team * T;
@@ -707,11 +813,11 @@ __device__ __forceinline__ void jk_team_body(const Src& src) {
         ci = lane / C::NFJ;
         cj = lane - ci * C::NFJ;
     }
-    int own_x = cart_lx(C::LI, ci) * C::SI, own_y = cart_ly(C::LI, ci) * C::SI, own_z = cart_lz(C::LI, ci) * C::SI;
+    int own_x = cart_lx(C::LI, ci) * L::SI, own_y = cart_ly(C::LI, ci) * L::SI, own_z = cart_lz(C::LI, ci) * L::SI;
     if (C::P == 2) {
-        own_x += cart_lx(C::LJ, cj) * C::SJ;
-        own_y += cart_ly(C::LJ, cj) * C::SJ;
-        own_z += cart_lz(C::LJ, cj) * C::SJ;
+        own_x += cart_lx(C::LJ, cj) * L::SJ;
+        own_y += cart_ly(C::LJ, cj) * L::SJ;
+        own_z += cart_lz(C::LJ, cj) * L::SJ;
     }
 
     __syncthreads();
@@ -769,7 +875,7 @@ __device__ __forceinline__ void jk_team_body(const Src& src) {
                             int r = u / 3, d = u - 3 * r;
                             float s, w;
                             rys_root_one_f<NR>(reinterpret_cast<const float*>(tab), pf.x, r, s, w);
-                            jk_unit_f<C>(pf, s, w, d, normf, dijf, dklf, g + u * C::GS);
+                            jk_unit_f<C, L::SI, L::SJ>(pf, s, w, d, normf, dijf, dklf, g + u * L::GS);
                         }
                     } else {
                         JKPrim p = jk_prim2(jk_pp(sg, q.prim_ij + ip), kc);
@@ -778,7 +884,7 @@ __device__ __forceinline__ void jk_team_body(const Src& src) {
                             double s, w;
                             if (S::SMEM_TAB) rys_root_one<NR>(tab, p.x, r, s, w);
                             else rys_root<NR>(sg.rys, p.x, r, s, w);
-                            jk_unit<C, R>(p, s, w, d, q.norm, ri, rj, rk, rl, g + u * C::GS);
+                            jk_unit<C, R, L::SI, L::SJ>(p, s, w, d, q.norm, ri, rj, rk, rl, g + u * L::GS);
                         }
                     }
                 }
@@ -786,9 +892,9 @@ __device__ __forceinline__ void jk_team_body(const Src& src) {
                 if (active) {
 #pragma unroll
                     for (int r = 0; r < NR; r++) {
-                        const R* gx = g + (3 * r) * C::GS;
-                        const R* gy = gx + C::GS;
-                        const R* gz = gy + C::GS;
+                        const R* gx = g + (3 * r) * L::GS;
+                        const R* gy = gx + L::GS;
+                        const R* gz = gy + L::GS;
                         if (C::P == 1) {
 #pragma unroll
                             for (int j = 0; j < C::NFJ; j++)
@@ -796,9 +902,9 @@ __device__ __forceinline__ void jk_team_body(const Src& src) {
                                 for (int k = 0; k < C::NFK; k++)
 #pragma unroll
                                     for (int l = 0; l < C::NFL; l++) {
-                                        int ox = cart_lx(C::LJ, j) * C::SJ + cart_lx(C::LK, k) * C::SK + cart_lx(C::LL, l);
-                                        int oy = cart_ly(C::LJ, j) * C::SJ + cart_ly(C::LK, k) * C::SK + cart_ly(C::LL, l);
-                                        int oz = cart_lz(C::LJ, j) * C::SJ + cart_lz(C::LK, k) * C::SK + cart_lz(C::LL, l);
+                                        int ox = cart_lx(C::LJ, j) * L::SJ + cart_lx(C::LK, k) * C::SK + cart_lx(C::LL, l);
+                                        int oy = cart_ly(C::LJ, j) * L::SJ + cart_ly(C::LK, k) * C::SK + cart_ly(C::LL, l);
+                                        int oz = cart_lz(C::LJ, j) * L::SJ + cart_lz(C::LK, k) * C::SK + cart_lz(C::LL, l);
                                         acc[(j * C::NFK + k) * C::NFL + l] +=
                                             gx[own_x + ox] * gy[own_y + oy] * gz[own_z + oz];
                                     }
