@@ -467,6 +467,10 @@ struct JKSeg {
     int pair_ij0, pair_kl0;  // first pair of each class in the pair arrays
     int prim_ij0, prim_kl0;  // first primitive pair of each class
     int nprim_ij, nprim_kl;
+    // primitive pairs are stored primitive-major within a class: primitive
+    // k of pair r at prim0 + k*pst + r (pst = pairs in the class), so the
+    // lanes of a warp (consecutive kl pairs) load them coalesced
+    int pst_ij, pst_kl;
     int nao, n_dm;
     const int* pair2bra;
     const int* pair2ket;

@@ -198,7 +198,7 @@ __device__ void jk_generic_body(const Src& src) {
             __syncthreads();
             for (int kp = 0; kp < npkl; kp++)
                 for (int ip = 0; ip < npij; ip++) {
-                    if (tid == 0) s_p = jk_prim2(jk_pp(sg, q.prim_ij + ip), jk_pp(sg, q.prim_kl + kp));
+                    if (tid == 0) s_p = jk_prim2(jk_pp(sg, q.prim_ij + ip * sg.pst_ij), jk_pp(sg, q.prim_kl + kp * sg.pst_kl));
                     __syncthreads();
                     if (tid < nr) rys_root_rt(sg.rys, nr, s_p.x, tid, s_rs[tid], s_rw[tid]);
                     __syncthreads();

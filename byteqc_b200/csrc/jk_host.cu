@@ -596,9 +596,11 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
     // the small differences P - R_i keep their relative precision
     std::vector<float> primf(6 * (size_t)(npp ? npp : 1));
     b->h_pnp.assign(std::max<size_t>(b->h_pair2bra.size(), 1), 0);
-    {
-        long long off = 0;
-        for (size_t p = 0; p < b->h_pair2bra.size(); p++) {
+    for (int c = 0; c < b->ncp; c++) {
+        // primitive-major within the class: primitive k of pair r at
+        // h_prim_locs[c] + k * (pairs in the class) + r
+        const int p0 = b->h_pair_locs[c], pst = b->h_pair_locs[c + 1] - p0;
+        for (int p = p0; p < p0 + pst; p++) {
             int ish = b->h_pair2bra[p], jsh = b->h_pair2ket[p];
             int npi = bas[ish * BAS_SLOTS + NPRIM_OF], npj = bas[jsh * BAS_SLOTS + NPRIM_OF];
             int li = bas[ish * BAS_SLOTS + ANG_OF], lj = bas[jsh * BAS_SLOTS + ANG_OF];
@@ -624,6 +626,7 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
                         if (kept == (pass == 0)) order.push_back({ip, jp});
                         if (pass == 0 && kept) b->h_pnp[p]++;
                     }
+            long long off = b->h_prim_locs[c] + (p - p0);
             for (const auto& pr : order) {
                 const int ip = pr.first, jp = pr.second;
                 {
@@ -643,7 +646,7 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
                     primf[4 * npp + off] = (float)(aj[jp] * (rj[1] - ri[1]) / aij);
                     primf[5 * npp + off] = (float)(aj[jp] * (rj[2] - ri[2]) / aij);
                 }
-                off++;
+                off += pst;
             }
         }
     }
@@ -788,6 +791,8 @@ static void fill_seg(const jk_basis* b, int cp_ij, int cp_kl, const long long* q
     s->prim_kl0 = b->h_prim_locs[cp_kl];
     s->nprim_ij = b->h_group_nprim[b->h_cls_gi[cp_ij]] * b->h_group_nprim[b->h_cls_gj[cp_ij]];
     s->nprim_kl = b->h_group_nprim[b->h_cls_gi[cp_kl]] * b->h_group_nprim[b->h_cls_gj[cp_kl]];
+    s->pst_ij = b->h_pair_locs[cp_ij + 1] - b->h_pair_locs[cp_ij];
+    s->pst_kl = b->h_pair_locs[cp_kl + 1] - b->h_pair_locs[cp_kl];
     s->nao = b->nao;
     s->n_dm = n_dm;
     s->pair2bra = b->d_pair2bra;

@@ -45,7 +45,7 @@ __device__ __forceinline__ int jk_find_row(const long long* __restrict__ qoff, i
 struct JKQuartet {
     int bij, bkl;          // global pair indices
     int i0, j0, k0, l0;    // first AO of each shell
-    int prim_ij, prim_kl;  // first primitive pair of ij and kl
+    int prim_ij, prim_kl;  // first primitive pair of ij and kl (stride sg.pst_ij, sg.pst_kl)
     int row, col;          // pair indices within the two classes
     double norm;
 };
@@ -60,8 +60,8 @@ __device__ __forceinline__ JKQuartet jk_quartet_at(const JKSeg& sg, int row, int
     q.j0 = __ldg(sg.pao + sg.npt + bij);
     q.k0 = __ldg(sg.pao + bkl);
     q.l0 = __ldg(sg.pao + sg.npt + bkl);
-    q.prim_ij = sg.prim_ij0 + row * sg.nprim_ij;
-    q.prim_kl = sg.prim_kl0 + col * sg.nprim_kl;
+    q.prim_ij = sg.prim_ij0 + row;  // primitive k at + k * sg.pst_ij
+    q.prim_kl = sg.prim_kl0 + col;
     q.row = row;
     q.col = col;
     // 2 pi^3 / sqrt(pi), halved on the ij == kl diagonal (g2e.c:41, g2e.cu:1025)
@@ -516,9 +516,9 @@ __device__ __forceinline__ void jk_thread_pass(const JKSeg& sg, const JKQuartet&
         JKPPF kn = jk_ppf(sg, q.prim_kl);
         for (int kp = 0; kp < npkl; kp++) {
             const JKPPF kc = kn;
-            if (kp + 1 < npkl) kn = jk_ppf(sg, q.prim_kl + kp + 1);  // next ket primitive, in flight
+            if (kp + 1 < npkl) kn = jk_ppf(sg, q.prim_kl + (kp + 1) * sg.pst_kl);  // next ket primitive, in flight
             for (int ip = 0; ip < npij; ip++) {
-                JKPrimF p = jk_prim_f2(jk_ppf(sg, q.prim_ij + ip), kc, ac);
+                JKPrimF p = jk_prim_f2(jk_ppf(sg, q.prim_ij + ip * sg.pst_ij), kc, ac);
                 float rs[NR], rw[NR];
                 rys_roots_all_f<NR>(tabf, p.x, rs, rw);
 #pragma unroll
@@ -537,9 +537,9 @@ __device__ __forceinline__ void jk_thread_pass(const JKSeg& sg, const JKQuartet&
         JKPP kn = jk_pp(sg, q.prim_kl);
         for (int kp = 0; kp < npkl; kp++) {
             const JKPP kc = kn;
-            if (kp + 1 < npkl) kn = jk_pp(sg, q.prim_kl + kp + 1);  // next ket primitive, in flight
+            if (kp + 1 < npkl) kn = jk_pp(sg, q.prim_kl + (kp + 1) * sg.pst_kl);  // next ket primitive, in flight
             for (int ip = 0; ip < npij; ip++) {
-                JKPrim p = jk_prim2(jk_pp(sg, q.prim_ij + ip), kc);
+                JKPrim p = jk_prim2(jk_pp(sg, q.prim_ij + ip * sg.pst_ij), kc);
                 double rs[NR], rw[NR];
                 rys_roots_all<NR>(tab, p.x, rs, rw);
 #pragma unroll
@@ -863,13 +863,13 @@ __device__ __forceinline__ void jk_team_body(const Src& src) {
             JKPP kc;
             JKPPF kcf;
             if (active) {
-                if constexpr (F32P) kcf = jk_ppf(sg, q.prim_kl + kp);
-                else kc = jk_pp(sg, q.prim_kl + kp);
+                if constexpr (F32P) kcf = jk_ppf(sg, q.prim_kl + kp * sg.pst_kl);
+                else kc = jk_pp(sg, q.prim_kl + kp * sg.pst_kl);
             }
             for (int ip = 0; ip < nprim_ij; ip++) {
                 if (active) {
                     if constexpr (F32P) {
-                        const JKPrimF pf = jk_prim_f2(jk_ppf(sg, q.prim_ij + ip), kcf, acf);
+                        const JKPrimF pf = jk_prim_f2(jk_ppf(sg, q.prim_ij + ip * sg.pst_ij), kcf, acf);
                         const float normf = (float)q.norm;
                         for (int u = lane; u < 3 * NR; u += T) {
                             int r = u / 3, d = u - 3 * r;
@@ -878,7 +878,7 @@ __device__ __forceinline__ void jk_team_body(const Src& src) {
                             jk_unit_f<C, L::SI, L::SJ>(pf, s, w, d, normf, dijf, dklf, g + u * L::GS);
                         }
                     } else {
-                        JKPrim p = jk_prim2(jk_pp(sg, q.prim_ij + ip), kc);
+                        JKPrim p = jk_prim2(jk_pp(sg, q.prim_ij + ip * sg.pst_ij), kc);
                         for (int u = lane; u < 3 * NR; u += T) {
                             int r = u / 3, d = u - 3 * r;
                             double s, w;
