@@ -36,14 +36,20 @@ WORKLOADS = {
     'h2o8-dz': (8, 9.0, 0, 'standin-cc-pvdz'),
     'h2o64-dz': (64, 18.0, 3, 'standin-cc-pvdz'),
     'h2o12-tzvp': (12, 10.5, 2, 'standin-def2-tzvp'),  # small case for ncu captures
+    # a 60-atom random-walk molecule (the kind of the batched workload)
+    'walk60-631gs': ('walk', 60, 11, 'standin-6-31g*'),
 }
 
 
 def make_workload(name):
     from byteqc_b200.gto import Mole, geom
     nw, box, seed, basis = WORKLOADS[name]
-    mol = Mole(atom=geom.water_cluster(nw, box=box, seed=seed),
-               basis=basis).build()
+    if nw == 'walk':
+        mol = Mole(atom=geom.random_walk_molecule(box, seed=seed),
+                   basis=basis).build()
+    else:
+        mol = Mole(atom=geom.water_cluster(nw, box=box, seed=seed),
+                   basis=basis).build()
     s = mol.intor('int1e_ovlp')
     dm = geom.scf_like_density(s, nocc=mol.nelectron // 2, seed=1)
     return mol, dm
@@ -554,7 +560,9 @@ def main():
         'ms_per_step': ms_step, 'higher_is_better': True, 'scaling': 'weak',
         'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
         'config': {'workload': args.workload,
-                   'molecule': '(H2O)%d' % WORKLOADS[args.workload][0],
+                   'molecule': ('random walk, %d atoms' % WORKLOADS[args.workload][1]
+                                if WORKLOADS[args.workload][0] == 'walk'
+                                else '(H2O)%d' % WORKLOADS[args.workload][0]),
                    'basis': WORKLOADS[args.workload][3],
                    'nao': int(nao0), 'nao_working': int(nao),
                    'parallelism': 'replicas' if world > 1 else 'single',

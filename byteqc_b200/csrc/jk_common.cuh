@@ -95,9 +95,9 @@ __device__ __forceinline__ void boys01(double x, double& f0, double& f1) {
         f0 = a0;
         f1 = a1;
     } else {
-        double sx = sqrt(x);
-        f0 = 0.88622692545275801365 * erf(sx) / sx;  // sqrt(pi)/2 erf(sqrt x)/sqrt x
-        f1 = (f0 - exp(-x)) / (2. * x);
+        const double rx = rsqrt(x), sx = x * rx;        // 1/sqrt(x), sqrt(x)
+        f0 = 0.88622692545275801365 * erf(sx) * rx;     // sqrt(pi)/2 erf(sqrt x)/sqrt x
+        f1 = (f0 - exp(-x)) * (0.5 * rx * rx);         // (F0 - e^-x) / (2x)
     }
 }
 

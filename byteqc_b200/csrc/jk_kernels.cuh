@@ -182,11 +182,13 @@ __device__ __forceinline__ JKPrim jk_prim2(const JKPP& b, const JKPP& k) {
         p.Q[d] = k.P[d];
     }
     p.AB = p.A + p.B;
-    p.iAB = 1. / p.AB;
+    // one reciprocal square root gives both 1/(A+B) and 1/sqrt(A+B)
+    const double rs = rsqrt(p.AB);
+    p.iAB = rs * rs;
     const double rho = p.A * p.B * p.iAB;
     const double dx = p.P[0] - p.Q[0], dy = p.P[1] - p.Q[1], dz = p.P[2] - p.Q[2];
     p.x = rho * (dx * dx + dy * dy + dz * dz);
-    p.sy = b.e * k.e * sqrt(p.iAB);
+    p.sy = b.e * k.e * rs;
     return p;
 }
 
