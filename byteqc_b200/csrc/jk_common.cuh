@@ -94,10 +94,16 @@ __device__ __forceinline__ void boys01(double x, double& f0, double& f1) {
         }
         f0 = a0;
         f1 = a1;
-    } else {
+    } else if (x < 40.) {
         const double rx = rsqrt(x), sx = x * rx;        // 1/sqrt(x), sqrt(x)
         f0 = 0.88622692545275801365 * erf(sx) * rx;     // sqrt(pi)/2 erf(sqrt x)/sqrt x
         f1 = (f0 - exp(-x)) * (0.5 * rx * rx);         // (F0 - e^-x) / (2x)
+    } else {
+        // asymptotic: erfc(sqrt 40) < 1e-18 and e^-40 / F0 < 3e-17, below the
+        // double rounding of the terms kept
+        const double rx = rsqrt(x);
+        f0 = 0.88622692545275801365 * rx;
+        f1 = f0 * (0.5 * rx * rx);
     }
 }
 
