@@ -101,6 +101,105 @@ def test_eri_vs_obara_saika_g_h():
         assert abs(a - b).max() <= 1e-12 * abs(b).max() + 1e-14, lq
 
 
+def _boys_series(m, x, digits=130):
+    """F_m(x) = e^-x sum_k (2x)^k / ((2m+1)(2m+3)...(2m+2k+1)), summed in
+    decimal arithmetic with enough digits for the cancellation at x = 200."""
+    from decimal import Decimal, getcontext
+    getcontext().prec = digits
+    X = Decimal(repr(float(x)))
+    term = Decimal(1) / Decimal(2 * m + 1)
+    tot = term
+    k = 0
+    while True:
+        k += 1
+        term = term * 2 * X / Decimal(2 * m + 2 * k + 1)
+        tot += term
+        if term < tot * Decimal(10) ** (-40):
+            break
+    return float(tot * (-X).exp())
+
+
+def test_boys_vs_high_precision_series():
+    """The Boys function used as the reference of the Rys moment test
+    against a high-precision series, m = 0..12, x in [0, 200]."""
+    from oracle.eri_os import boys
+    for m in range(13):
+        for x in (0.0, 1e-3, 0.3, 1.0, 4.7, 12.0, 33.0, 60.0, 119.0, 200.0):
+            ref = _boys_series(m, x)
+            got = boys(m, x)
+            assert abs(got - ref) <= 1e-13 * ref, (m, x, got, ref)
+
+
+def _shifted(atoms, shift=(0., 0., 0.), rot=None):
+    out = []
+    for sym, xyz in atoms:
+        v = np.asarray(xyz, dtype=float)
+        if rot is not None:
+            v = rot @ v
+        out.append((sym, tuple(v + np.asarray(shift))))
+    return out
+
+
+def test_eri_symmetry_and_invariance():
+    """Contracted shell quartets of the oracle: the 8-fold permutation
+    symmetry, invariance under a translation of the molecule, and the
+    transformation of a (pp|pp) block under a rotation."""
+    import oracle
+    from oracle import hf_oracle
+    atoms = geom.water_cluster(2, box=4.0, seed=2)
+
+    def pmol(at):
+        mol = Mole(atom=at, basis='standin-def2-tzvp').build()
+        return hf_oracle.VHFOpt(mol).build().mol
+    pm = pmol(atoms)
+    pt = pmol(_shifted(atoms, shift=(1.3, -0.7, 2.1)))
+    ls = pm._bas[:, 1]
+    rng = np.random.default_rng(5)
+    by_l = {l: np.flatnonzero(ls == l) for l in range(4)}
+    for lq in [(3, 2, 1, 0), (2, 1, 2, 1), (1, 1, 0, 0), (3, 3, 1, 1)]:
+        i, j, k, l = [int(rng.choice(by_l[x])) for x in lq]
+        a = oracle.eri_shells(pm, i, j, k, l)
+        tol = 1e-13 * abs(a).max() + 1e-15
+        assert abs(a - oracle.eri_shells(pm, j, i, k, l).transpose(1, 0, 2, 3)).max() <= tol
+        assert abs(a - oracle.eri_shells(pm, i, j, l, k).transpose(0, 1, 3, 2)).max() <= tol
+        assert abs(a - oracle.eri_shells(pm, k, l, i, j).transpose(2, 3, 0, 1)).max() <= tol
+        assert abs(a - oracle.eri_shells(pt, i, j, k, l)).max() <= 1e-12 * abs(a).max() + 1e-15
+    # rotation: Cartesian p components transform as vectors
+    th = 0.7
+    R = np.array([[np.cos(th), -np.sin(th), 0.], [np.sin(th), np.cos(th), 0.], [0., 0., 1.]])
+    ax = np.array([1., 2., 2.]) / 3.
+    K = np.array([[0, -ax[2], ax[1]], [ax[2], 0, -ax[0]], [-ax[1], ax[0], 0]])
+    R = R @ (np.eye(3) + np.sin(0.4) * K + (1 - np.cos(0.4)) * K @ K)
+    pr = pmol(_shifted(atoms, rot=R))
+    p_sh = by_l[1]
+    i, j, k, l = (int(p_sh[0]), int(p_sh[-1]), int(p_sh[1]), int(p_sh[-2]))
+    a = oracle.eri_shells(pm, i, j, k, l)
+    b = oracle.eri_shells(pr, i, j, k, l)
+    ra = np.einsum('ai,bj,ck,dl,ijkl->abcd', R, R, R, R, a)
+    assert abs(ra - b).max() <= 1e-12 * abs(a).max()
+
+
+def test_jk_linearity_and_symmetry():
+    """Oracle J/K as operators: J(D) and K(D) symmetric for symmetric D,
+    linear in D, and tr(D1 J(D2)) = tr(D2 J(D1)) (likewise K)."""
+    from oracle import hf_oracle
+    mol = Mole(atom=geom.water_cluster(2, box=5.0, seed=3),
+               basis='standin-cc-pvdz').build()
+    opt = hf_oracle.VHFOpt(mol).build()
+    rng = np.random.default_rng(9)
+    d = rng.random((2, mol.nao, mol.nao))
+    d = d + d.transpose(0, 2, 1)
+    dm = np.stack([d[0], d[1], 0.3 * d[0] - 1.7 * d[1]])
+    vj, vk = hf_oracle.get_jk(mol, dm, vhfopt=opt)
+    sc = max(abs(vj).max(), abs(vk).max())
+    for v in (vj, vk):
+        assert abs(v - v.transpose(0, 2, 1)).max() <= 1e-12 * sc
+        assert abs(v[2] - (0.3 * v[0] - 1.7 * v[1])).max() <= 1e-11 * sc
+        t12 = np.sum(d[0] * v[1])
+        t21 = np.sum(d[1] * v[0])
+        assert abs(t12 - t21) <= 1e-11 * abs(t12)
+
+
 def test_jk_vs_full_eri_tensor():
     """Oracle get_jk (screened, binned, 8-fold symmetric loop) against J and K
     contracted from the full ERI tensor of the working basis."""
