@@ -204,6 +204,24 @@ def test_get_jk_vs_oracle_larger():
     _close(vk, rk)
 
 
+def test_get_jk_water8_dz_vs_oracle():
+    """The (H2O)8 / cc-pVDZ workload (9 A cube, seed 0, SCF-like density) at
+    full size against the oracle, in FP64 and in the mixed mode (its error
+    bounded by the cutoff)."""
+    from byteqc_b200.cuobc.scf import hf
+    from oracle import hf_oracle
+    mol = _mol(8, 'standin-cc-pvdz', 9.0, seed=0)
+    dm = geom.scf_like_density(mol.intor('int1e_ovlp'),
+                               nocc=mol.nelectron // 2, seed=1)
+    opt = hf._VHFOpt(mol).build()
+    vj, vk = hf.get_jk(mol, dm, vhfopt=opt)
+    rj, rk = hf_oracle.get_jk(mol, dm)
+    _close(vj, rj)
+    _close(vk, rk)
+    mj, mk = hf.get_jk(mol, dm, vhfopt=opt, fp32_cutoff=1e-6)
+    assert max(abs(mj - rj).max(), abs(mk - rk).max()) < 1e-4
+
+
 @pytest.mark.parametrize('case', ['h2o-dz', 'h2o2-tzvp', 'walk6-631gs'])
 def test_get_jk_vs_golden(case):
     """The engine against the committed golden J/K (tests/golden)."""
