@@ -592,11 +592,6 @@ struct JKThreadMinBlocks {
 
 template <class C, typename R, class Src>
 __device__ __forceinline__ void jk_thread_body(const Src& src, double* jk_tab) {
-    if constexpr (JKF32Prim<C, R>::value)
-        rys_table_to_smem_f<C::NROOTS>(src.first().rys, reinterpret_cast<float*>(jk_tab));
-    else
-        rys_table_to_smem<C::NROOTS>(src.first().rys, jk_tab);
-    __syncthreads();
     // each warp takes a contiguous chunk of tasks (a multiple of 32); lane i
     // does tasks i, i+32, ... of it, so a warp covers consecutive kl of a row
     const long long total = src.total();
@@ -604,6 +599,14 @@ __device__ __forceinline__ void jk_thread_body(const Src& src, double* jk_tab) {
     const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
     const long long wid = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const long long chunk = (((total + nwarps - 1) / nwarps) + 31) & ~31LL;
+    // the grid is sized for the unscreened task count: a block without any
+    // screened task leaves before it loads the Rys table (block-uniform test)
+    if ((long long)blockIdx.x * (blockDim.x >> 5) * chunk >= total) return;
+    if constexpr (JKF32Prim<C, R>::value)
+        rys_table_to_smem_f<C::NROOTS>(src.first().rys, reinterpret_cast<float*>(jk_tab));
+    else
+        rys_table_to_smem<C::NROOTS>(src.first().rys, jk_tab);
+    __syncthreads();
     long long t = wid * chunk + lane;
     const long long tend = min(total, (wid + 1) * chunk);
     if (t >= tend) return;
@@ -800,6 +803,14 @@ __device__ __forceinline__ void jk_team_body(const Src& src) {
     double* part = reinterpret_cast<double*>(g);  // digestion partials reuse the 2D-block space
     double* buf = reinterpret_cast<double*>(gbase + jk_team_gbytes<C, R>()) + (size_t)team * S::BWORDS;
     const JKSeg& sg0 = src.first();
+    // each team takes a contiguous chunk of tasks; every team of the block
+    // runs the same number of iterations (the block synchronises inside).
+    // The grid is sized for the unscreened task count: a block whose first
+    // team has no screened task leaves before it loads the Rys table.
+    const long long total = src.total();
+    const long long nteams = (long long)gridDim.x * S::QPB;
+    const long long chunk = (total + nteams - 1) / nteams;
+    if ((long long)blockIdx.x * S::QPB * chunk >= total) return;
     // FP32 quartets at low order: float prefactors, nodes and weights (the
     // table copy in shared memory is then single precision)
     constexpr bool F32P = JKF32Prim<C, R>::value && S::SMEM_TAB;
@@ -823,13 +834,8 @@ __device__ __forceinline__ void jk_team_body(const Src& src) {
     }
 
     __syncthreads();
-    const long long total = src.total();
     const int nprim_ij = sg0.nprim_ij, nprim_kl = sg0.nprim_kl;  // uniform within a launch
-    // each team takes a contiguous chunk of tasks; every team of the block
-    // runs the same number of iterations (the block synchronises inside)
-    const long long nteams = (long long)gridDim.x * S::QPB;
     const long long tid = (long long)blockIdx.x * S::QPB + team;
-    const long long chunk = (total + nteams - 1) / nteams;
     const long long tbeg = tid * chunk, tend = min(total, tbeg + chunk);
     typename Src::Cursor cur;
     if (tbeg < tend) cur.init(src, tbeg);
