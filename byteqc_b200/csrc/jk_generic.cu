@@ -315,6 +315,135 @@ static cudaError_t jk_launch_generic_batch(const JKSeg* segs, const long long* s
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// ERI tensor fill (the reference's GINTfill_int2e, gint/nr_fill_ao_ints.cu:
+// 493-549, kernels gint/g2e.cu:1160-1605): for every screened quartet of a
+// class pair, eri[(a-o0)*s0 + (b-o1)*s1 + (c-o2)*s2 + (d-o3)*s3] += (ab|cd)
+// over the Cartesian components a, b, c, d of the four shells (AO indices of
+// the working basis).  Every class up to (hh|hh); one CTA per quartet; the
+// quartet's integrals are summed over primitives and roots in a shared-memory
+// chunk of up to JK_FILL_CHUNK elements (classes with more components run
+// the primitive loop once per chunk), then added to the tensor.  The
+// integrals carry no 1/2 on the ij == kl diagonal (that factor belongs to
+// the J/K digestion); pairs on the diagonal of a shell carry the basis
+// handle's diagonal factor, as the reference's pair data do.
+// ---------------------------------------------------------------------------
+#define JK_FILL_CHUNK 4096
+
+struct JKFillOut {
+    double* eri;
+    long long st[4];
+    int off[4];
+};
+
+__global__ void __launch_bounds__(JK_GEN_THREADS) jk_fill_kernel(const __grid_constant__ JKSeg sg,
+                                                                 const long long* __restrict__ task0,
+                                                                 const JKFillOut out) {
+    extern __shared__ __align__(16) double gsm[];
+    double* gI = gsm;                     // 3 x JK_GEN_GS: the blocks of one root
+    double* acc = gI + 3 * JK_GEN_GS;     // JK_FILL_CHUNK integrals of the quartet
+    double* wk = acc + JK_FILL_CHUNK;     // 3 x JK_GEN_W: recursion scratch of threads 0-2
+    __shared__ JKQuartet s_q;
+    __shared__ double s_c[12];
+    __shared__ JKPrim s_p;
+    __shared__ double s_rs[JK_GEN_NR], s_rw[JK_GEN_NR];
+    __shared__ int s_ex[4][JK_GEN_NF][3];
+    const int tid = threadIdx.x;
+    const long long total = task0[1];
+    const long long chunk = (total + gridDim.x - 1) / gridDim.x;
+    const long long tbeg = (long long)blockIdx.x * chunk;
+    const long long tend = min(total, tbeg + chunk);
+    if (tbeg >= tend) return;
+    const int li = sg.ls[0], lj = sg.ls[1], lk = sg.ls[2], ll = sg.ls[3];
+    const int nfi = ncart(li), nfj = ncart(lj), nfk = ncart(lk), nfl = ncart(ll);
+    const int nf = nfi * nfj * nfk * nfl;
+    const int nr = (li + lj + lk + ll) / 2 + 1;
+    const int SK = ll + 1, SJ = (lk + 1) * SK, SI = (lj + 1) * SJ;
+    for (int sh = 0; sh < 4; sh++) jk_cart_table(sg.ls[sh], s_ex[sh]);
+    JKTaskCursor cur;
+    if (tid == 0) cur.init(sg, tbeg);
+    for (long long t = tbeg; t < tend; t++) {
+        if (tid == 0) {
+            const int col = cur.seek(sg, t);
+            s_q = jk_quartet_at(sg, cur.row, col);
+            load_pair_centres(sg, s_q.bij, s_c, s_c + 3);
+            load_pair_centres(sg, s_q.bkl, s_c + 6, s_c + 9);
+        }
+        __syncthreads();
+        const JKQuartet q = s_q;
+        const int npij = sg.pnp ? __ldg(sg.pnp + q.bij) : sg.nprim_ij;
+        const int npkl = sg.pnp ? __ldg(sg.pnp + q.bkl) : sg.nprim_kl;
+        for (int c0 = 0; c0 < nf; c0 += JK_FILL_CHUNK) {
+            const int c1 = min(nf, c0 + JK_FILL_CHUNK);
+            for (int e = c0 + tid; e < c1; e += JK_GEN_THREADS) acc[e - c0] = 0.;
+            for (int kp = 0; kp < npkl; kp++)
+                for (int ip = 0; ip < npij; ip++) {
+                    if (tid == 0)
+                        s_p = jk_prim2(jk_pp(sg, q.prim_ij + ip * sg.pst_ij), jk_pp(sg, q.prim_kl + kp * sg.pst_kl));
+                    __syncthreads();
+                    if (tid < nr) rys_root_rt(sg.rys, nr, s_p.x, tid, s_rs[tid], s_rw[tid]);
+                    __syncthreads();
+                    for (int r = 0; r < nr; r++) {
+                        if (tid < 3)
+                            jk_unit_rt(s_p, s_rs[r], s_rw[r], tid, JK_FAC, s_c, s_c + 3, s_c + 6, s_c + 9, li, lj, lk,
+                                       ll, wk + tid * JK_GEN_W, gI + tid * JK_GEN_GS);
+                        __syncthreads();
+                        for (int e = c0 + tid; e < c1; e += JK_GEN_THREADS) {
+                            int x = e;
+                            const int l = x % nfl;
+                            x /= nfl;
+                            const int k = x % nfk;
+                            x /= nfk;
+                            const int j = x % nfj;
+                            const int i = x / nfj;
+                            double v = 1.;
+                            for (int d = 0; d < 3; d++)
+                                v *= gI[d * JK_GEN_GS + s_ex[0][i][d] * SI + s_ex[1][j][d] * SJ + s_ex[2][k][d] * SK +
+                                        s_ex[3][l][d]];
+                            acc[e - c0] += v;
+                        }
+                        __syncthreads();  // the next root rebuilds the blocks
+                    }
+                }
+            for (int e = c0 + tid; e < c1; e += JK_GEN_THREADS) {
+                int x = e;
+                const int l = x % nfl;
+                x /= nfl;
+                const int k = x % nfk;
+                x /= nfk;
+                const int j = x % nfj;
+                const int i = x / nfj;
+                const long long o = (long long)(q.i0 + i - out.off[0]) * out.st[0] +
+                                    (long long)(q.j0 + j - out.off[1]) * out.st[1] +
+                                    (long long)(q.k0 + k - out.off[2]) * out.st[2] +
+                                    (long long)(q.l0 + l - out.off[3]) * out.st[3];
+                atomicAdd(out.eri + o, acc[e - c0]);
+            }
+            __syncthreads();  // acc is reused by the next chunk / quartet
+        }
+    }
+}
+
+static constexpr size_t JK_FILL_SMEM = (3 * JK_GEN_GS + JK_FILL_CHUNK + 3 * JK_GEN_W) * sizeof(double);
+
+cudaError_t jk_launch_fill(const JKSeg& seg, const long long* task0, long long max_tasks, int nsm, double* eri,
+                           const long long* strides, const int* offsets, cudaStream_t st) {
+    if (max_tasks <= 0) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(jk_fill_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)JK_FILL_SMEM);
+    if (e != cudaSuccess) return e;
+    JKFillOut out;
+    out.eri = eri;
+    for (int a = 0; a < 4; a++) {
+        out.st[a] = strides[a];
+        out.off[a] = offsets[a];
+    }
+    const long long cap = (long long)nsm * 2;  // two 77 KB CTAs per SM
+    const int blocks = (int)(max_tasks < cap ? max_tasks : cap);
+    jk_fill_kernel<<<blocks, JK_GEN_THREADS, JK_FILL_SMEM, st>>>(seg, task0, out);
+    return cudaGetLastError();
+}
+
 // every class with a shell above f runs the generic kernel, in FP64 also for
 // the FP32 part of the mixed mode
 void jk_register_generic(JKTables* T) {

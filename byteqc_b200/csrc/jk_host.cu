@@ -954,6 +954,55 @@ extern "C" int jk_build_class_pair(jk_basis_t* b, double* vj, double* vk, const 
     return JK_OK;
 }
 
+// ERI tensor of one class pair (jk_generic.cu)
+cudaError_t jk_launch_fill(const JKSeg& seg, const long long* task0, long long max_tasks, int nsm, double* eri,
+                           const long long* strides, const int* offsets, cudaStream_t st);
+
+extern "C" int jk_fill_int2e(jk_basis_t* b, double* eri, int nao, const int* strides, const int* ao_offsets,
+                             const int* bins_locs_ij, const int* bins_locs_kl, int nbins, int cp_ij, int cp_kl,
+                             void* stream) {
+    if (!b || !eri || !strides || !ao_offsets || !bins_locs_ij || !bins_locs_kl || nbins <= 0)
+        return set_err(JK_ERR_ARG, "jk_fill_int2e: invalid arguments");
+    if (nao != b->nao) return set_err(JK_ERR_ARG, "nao %d does not match the basis (%d)", nao, b->nao);
+    if (cp_ij < 0 || cp_ij >= b->ncp || cp_kl < 0 || cp_kl > cp_ij) return set_err(JK_ERR_ARG, "bad class pair");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int n_ij = b->h_pair_locs[cp_ij + 1] - b->h_pair_locs[cp_ij];
+    // kl bin kb pairs with ij in [bins_ij[0], bins_ij[nbins - kb]): row ij (in
+    // bin sij) keeps kl < bins_kl[nbins - sij] (nr_fill_ao_ints.cu:519-545)
+    if ((size_t)n_ij + 1 > b->h_qoff1_cap) {
+        if (b->h_qoff1) cudaFreeHost(b->h_qoff1);
+        CUDA_TRY(cudaMallocHost(&b->h_qoff1, sizeof(long long) * (n_ij + 1)));
+        b->h_qoff1_cap = n_ij + 1;
+    }
+    CUDA_TRY(cudaStreamSynchronize(st));
+    long long* qo = b->h_qoff1;
+    qo[0] = 0;
+    int sij = 0;
+    long long tot = 0;
+    for (int ij = 0; ij < n_ij; ij++) {
+        while (sij < nbins && ij >= bins_locs_ij[sij + 1]) sij++;
+        long long cnt = 0;
+        if (ij >= bins_locs_ij[0] && sij < nbins && bins_locs_kl[0] == 0) cnt = bins_locs_kl[nbins - sij];
+        tot += cnt;
+        qo[ij + 1] = tot;
+    }
+    if (n_ij + 1 > b->qoff1_cap) {
+        cudaFree(b->d_qoff1);
+        CUDA_TRY(cudaMalloc(&b->d_qoff1, sizeof(long long) * (n_ij + 1)));
+        b->qoff1_cap = n_ij + 1;
+    }
+    CUDA_TRY(cudaMemcpyAsync(b->d_qoff1, qo, sizeof(long long) * (n_ij + 1), cudaMemcpyHostToDevice, st));
+    long long t0[2] = {0, tot};
+    CUDA_TRY(cudaMemcpyAsync(b->d_task01, t0, sizeof(t0), cudaMemcpyHostToDevice, st));
+    JKSeg seg;
+    fill_seg(b, cp_ij, cp_kl, b->d_qoff1, n_ij, nullptr, 0, nullptr, nullptr, &seg);
+    long long s64[4];
+    for (int a = 0; a < 4; a++) s64[a] = strides[a];
+    CUDA_TRY(jk_launch_fill(seg, b->d_task01, tot, b->nsm, eri, s64, ao_offsets, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return JK_OK;
+}
+
 // row-major C[M,N] = alpha op(A) op(B) + beta C through column-major cuBLAS
 static cublasStatus_t gemm_rm(cublasHandle_t h, bool ta, bool tb, int M, int N, int K, double alpha,
                               const double* A, int lda, const double* B, int ldb, double beta, double* C, int ldc) {

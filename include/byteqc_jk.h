@@ -80,6 +80,21 @@ int jk_build_class_pair(jk_basis_t *basis, double *vj, double *vk, const double 
                         void *stream);
 
 /*
+ * ERI tensor of one class pair, same contract as GINTfill_int2e
+ * (cuobc/lib/gint/nr_fill_ao_ints.cu:493-549): for every (ij, kl) the host
+ * bins keep (kl bin b with ij bins below nbins - b, no triangle restriction
+ * on a diagonal class pair), eri[(a - o[0])*s[0] + (b - o[1])*s[1] +
+ * (c - o[2])*s[2] + (d - o[3])*s[3]] += (ab|cd) over the Cartesian
+ * functions of the four shells; eri is a device buffer, strides s[4] and AO
+ * offsets o[4] (working-basis AO indices) host arrays.  Pairs on the
+ * diagonal of a shell carry the basis's diagonal factor (1 with
+ * diag_block_with_triu, else 1/2), as the reference's pair data do.  Every
+ * class up to (hh|hh).
+ */
+int jk_fill_int2e(jk_basis_t *basis, double *eri, int nao, const int *strides, const int *ao_offsets,
+                  const int *bins_locs_ij, const int *bins_locs_kl, int nbins, int cp_ij, int cp_kl, void *stream);
+
+/*
  * Same computation and buffer contract as jk_build_class_pair, for callers
  * that must not allocate device memory while they run (a serving process or
  * host framework that owns all GPU memory through its own pool and cannot
