@@ -213,6 +213,26 @@ def bench_serve(args, torch):
     return out
 
 
+def bench_int4c(args, torch, timed):
+    """The dense ERI tensor of (H2O)2 / cc-pVDZ in the working basis through
+    int4c.get_int4c (the fill kernels of every class pair plus the eight
+    permuted block copies), CUDA-event timed."""
+    from byteqc_b200.cuobc.lib import int4c
+    from byteqc_b200.cuobc.scf.hf import _VHFOpt
+    from byteqc_b200.gto import Mole, geom
+    mol = Mole(atom=geom.water_cluster(2, box=5.0, seed=0),
+               basis='standin-cc-pvdz').build()
+    opt = _VHFOpt(mol).build(diag_block_with_triu=True)
+    int4c.get_int4c(mol, vhfopt=opt)
+    ms = timed(lambda: int4c.get_int4c(mol, vhfopt=opt), 2)
+    n = opt.nao
+    npair = n * (n + 1) // 2
+    return {'workload': '(H2O)2 standin-cc-pvdz, working basis',
+            'nao': n, 'ms': ms, 'tensor_gb': 8. * n ** 4 / 1e9,
+            'unique_integrals_per_s': npair * (npair + 1) // 2 / (ms * 1e-3),
+            'tensor_write_gbs': 8. * n ** 4 / (ms * 1e-3) / 1e9}
+
+
 def ncart(l):
     return (l + 1) * (l + 2) // 2
 
@@ -397,6 +417,8 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--workload', default='h2o32-tzvp', choices=sorted(WORKLOADS))
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-int4c', action='store_true',
+                    help='skip the ERI-tensor fill measurement')
     ap.add_argument('--profile-builds', type=int, default=0,
                     help='only run this many jk_build calls of the workload '
                          '(FP64, or mixed with --fp32-cutoff > 0 given '
@@ -593,6 +615,8 @@ def main():
         line['sweep'] = bench_sweep(args, torch, timed)
     if args.serve_requests > 0 and world == 1:
         line['serve'] = bench_serve(args, torch)
+    if not args.no_int4c and world == 1:
+        line['int4c'] = bench_int4c(args, torch, timed)
     if ms_mixed is not None:
         line['mixed'] = {'fp32_cutoff': args.fp32_cutoff,
                          'value': world * 1e3 / ms_mixed, 'unit': 'builds/s',
