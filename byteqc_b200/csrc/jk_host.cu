@@ -494,7 +494,10 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
         for (int s = s0; s < s1; s++)
             if (bas[s * BAS_SLOTS + ANG_OF] != l || bas[s * BAS_SLOTS + NPRIM_OF] != np)
                 return set_err(JK_ERR_ARG, "group %d mixes (l, nprim)", g);
-        if (g > 0 && l < b->h_group_l[g - 1]) return set_err(JK_ERR_ARG, "groups must be sorted by l");
+        // groups may come in any l order (the density-fitting basis of
+        // int3c concatenates molecule, exponent-0 shell and auxiliary
+        // basis); the J/K class launches exist for classes whose bra and
+        // ket are ordered by l, others report JK_ERR_UNSUPPORTED at build
         b->h_group_l.push_back(l);
         b->h_group_nprim.push_back(np);
     }
@@ -964,7 +967,9 @@ extern "C" int jk_fill_int2e(jk_basis_t* b, double* eri, int nao, const int* str
     if (!b || !eri || !strides || !ao_offsets || !bins_locs_ij || !bins_locs_kl || nbins <= 0)
         return set_err(JK_ERR_ARG, "jk_fill_int2e: invalid arguments");
     if (nao != b->nao) return set_err(JK_ERR_ARG, "nao %d does not match the basis (%d)", nao, b->nao);
-    if (cp_ij < 0 || cp_ij >= b->ncp || cp_kl < 0 || cp_kl > cp_ij) return set_err(JK_ERR_ARG, "bad class pair");
+    // any two class pairs (the two-centre metric of int3c.get_int2c pairs
+    // auxiliary classes in both orders)
+    if (cp_ij < 0 || cp_ij >= b->ncp || cp_kl < 0 || cp_kl >= b->ncp) return set_err(JK_ERR_ARG, "bad class pair");
     cudaStream_t st = (cudaStream_t)stream;
     const int n_ij = b->h_pair_locs[cp_ij + 1] - b->h_pair_locs[cp_ij];
     // kl bin kb pairs with ij in [bins_ij[0], bins_ij[nbins - kb]): row ij (in

@@ -347,6 +347,26 @@ class Mole:
         return m
 
 
+def conc_mol(m1, m2):
+    """One molecule holding the atoms and shells of ``m1`` followed by those
+    of ``m2`` (PySCF's gto.conc_mol): ``m2``'s atom indices and environment
+    pointers are shifted past ``m1``'s."""
+    m = m1.copy()
+    off = len(m1._env)
+    atm2 = m2._atm.copy()
+    atm2[:, PTR_COORD] += off
+    atm2[:, PTR_ZETA] += off
+    bas2 = m2._bas.copy()
+    bas2[:, ATOM_OF] += m1.natm
+    bas2[:, PTR_EXP] += off
+    bas2[:, PTR_COEFF] += off
+    m._atm = np.vstack([m1._atm, atm2]).astype(np.int32)
+    m._bas = np.vstack([m1._bas, bas2]).astype(np.int32)
+    m._env = np.concatenate([m1._env, m2._env])
+    m.cart = m1.cart
+    return m
+
+
 def _parse_atom_string(s):
     out = []
     for line in s.replace(';', '\n').splitlines():

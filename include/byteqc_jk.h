@@ -11,7 +11,11 @@
  * Working basis: the decontracted Cartesian basis with shells sorted into
  * groups of equal (l, nprim), exactly as the reference's _VHFOpt.build
  * prepares it (cuobc/scf/hf.py:288-330, 481-564).  Angular momentum up to h
- * (l = 5), as the reference's GPU kernels.
+ * (l = 5), as the reference's GPU kernels.  The J/K entries need the groups
+ * in increasing l (classes out of that order report JK_ERR_UNSUPPORTED);
+ * jk_fill_int2e takes them in any order (the density-fitting basis of
+ * cuobc/lib/int3c.py:208-264 appends an exponent-0 s shell and the
+ * auxiliary basis after the molecule's shells).
  */
 #ifndef BYTEQC_JK_H
 #define BYTEQC_JK_H
@@ -83,7 +87,7 @@ int jk_build_class_pair(jk_basis_t *basis, double *vj, double *vk, const double 
  * ERI tensor of one class pair, same contract as GINTfill_int2e
  * (cuobc/lib/gint/nr_fill_ao_ints.cu:493-549): for every (ij, kl) the host
  * bins keep (kl bin b with ij bins below nbins - b, no triangle restriction
- * on a diagonal class pair), eri[(a - o[0])*s[0] + (b - o[1])*s[1] +
+ * on a diagonal class pair; cp_kl may exceed cp_ij), eri[(a - o[0])*s[0] + (b - o[1])*s[1] +
  * (c - o[2])*s[2] + (d - o[3])*s[3]] += (ab|cd) over the Cartesian
  * functions of the four shells; eri is a device buffer, strides s[4] and AO
  * offsets o[4] (working-basis AO indices) host arrays.  Pairs on the
