@@ -233,6 +233,39 @@ def bench_int4c(args, torch, timed):
             'tensor_write_gbs': 8. * n ** 4 / (ms * 1e-3) / 1e9}
 
 
+# even-tempered stand-in auxiliary basis for the density-fitting measurement
+# (no fitting basis data is available offline)
+DF_AUX = {'O': [[0, [8.0, 1.0]], [0, [2.0, 1.0]], [0, [0.5, 1.0]],
+                [1, [3.0, 1.0]], [1, [0.8, 1.0]], [2, [1.5, 1.0]],
+                [3, [1.1, 1.0]]],
+          'H': [[0, [3.0, 1.0]], [0, [0.6, 1.0]], [1, [1.0, 1.0]]]}
+
+
+def bench_df(args, torch, timed):
+    """Density-fitting integrals of (H2O)8 / cc-pVDZ with the stand-in
+    auxiliary basis: every (ij|P) block of int3c.get_int3c plus the metric
+    factor of get_int2c, CUDA-event timed."""
+    from byteqc_b200.cuobc.lib import int3c
+    from byteqc_b200.gto import Mole, geom
+    atoms = geom.water_cluster(8, box=9.0, seed=0)
+    mol = Mole(atom=atoms, basis='standin-cc-pvdz').build()
+    aux = Mole(atom=atoms, basis=DF_AUX).build()
+    opt = int3c.VHFOpt3c(mol, aux, 'int3c2e').build()
+
+    def run():
+        for cp in range(len(opt.log_qs)):
+            for ca in range(len(opt.aux_log_qs)):
+                int3c.get_int3c(cp, ca, opt)
+        int3c.get_int2c(opt)
+    run()
+    ms = timed(run, 2)
+    nao, naux = int(opt.ao_loc[-1]), int(opt.aux_ao_loc[-1])
+    return {'workload': '(H2O)8 standin-cc-pvdz, even-tempered stand-in '
+                        'auxiliary basis, working bases',
+            'nao': nao, 'naux': naux, 'ms': ms,
+            'int3c_per_s': nao * (nao + 1) // 2 * naux / (ms * 1e-3)}
+
+
 def ncart(l):
     return (l + 1) * (l + 2) // 2
 
@@ -418,7 +451,7 @@ def main():
     ap.add_argument('--workload', default='h2o32-tzvp', choices=sorted(WORKLOADS))
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-int4c', action='store_true',
-                    help='skip the ERI-tensor fill measurement')
+                    help='skip the ERI-tensor fill and density-fitting measurements')
     ap.add_argument('--profile-builds', type=int, default=0,
                     help='only run this many jk_build calls of the workload '
                          '(FP64, or mixed with --fp32-cutoff > 0 given '
@@ -617,6 +650,7 @@ def main():
         line['serve'] = bench_serve(args, torch)
     if not args.no_int4c and world == 1:
         line['int4c'] = bench_int4c(args, torch, timed)
+        line['df'] = bench_df(args, torch, timed)
     if ms_mixed is not None:
         line['mixed'] = {'fp32_cutoff': args.fp32_cutoff,
                          'value': world * 1e3 / ms_mixed, 'unit': 'builds/s',
