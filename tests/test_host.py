@@ -93,3 +93,49 @@ def test_one_electron_analytic():
     mol = Mole(atom=[('H', (0, 0, 0))], basis={'H': [[0, [a, 1.0]]]}).build()
     assert abs(mol.intor('int1e_kin')[0, 0] - 1.5 * a) < 1e-13
     assert abs(mol.intor('int1e_nuc')[0, 0] + 2 * np.sqrt(2 * a / np.pi)) < 1e-13
+
+
+def test_conc_mol_keeps_both_molecules():
+    """conc_mol (the concatenated basis of the density-fitting integrals):
+    the second molecule's shells keep their exponents, coefficients and
+    centres after the pointer shift."""
+    from byteqc_b200.gto import mole as gmole
+    a = Mole(atom=geom.water_cluster(1, box=4.0, seed=1),
+             basis='standin-cc-pvdz').build()
+    b = Mole(atom=geom.water_cluster(2, box=5.0, seed=2),
+             basis='standin-6-31g*').build()
+    c = gmole.conc_mol(a, b)
+    assert c.nbas == a.nbas + b.nbas and c.natm == a.natm + b.natm
+    assert c.nao_nr(cart=True) == a.nao_nr(cart=True) + b.nao_nr(cart=True)
+    coords = c.atom_coords()
+    for ib in range(b.nbas):
+        jb = a.nbas + ib
+        assert np.array_equal(c.bas_exp(jb), b.bas_exp(ib))
+        assert np.array_equal(c.bas_ctr_coeff(jb), b.bas_ctr_coeff(ib))
+        assert c.bas_angular(jb) == b.bas_angular(ib)
+        ia = c._bas[jb, gmole.ATOM_OF]
+        assert np.array_equal(coords[ia], b.atom_coords()[b._bas[ib, gmole.ATOM_OF]])
+    for ib in range(a.nbas):
+        assert np.array_equal(c.bas_exp(ib), a.bas_exp(ib))
+
+
+def test_df_basis_helpers():
+    """Class-pair enumeration, the exponent-0 shell and the (l, nprim)
+    grouping of the density-fitting basis."""
+    from byteqc_b200.cuobc.lib import int3c, int4c
+    for gi in range(12):
+        for gj in range(gi + 1):
+            assert int4c.ind2pair(gi * (gi + 1) // 2 + gj) == (gi, gj)
+    fake = int3c.make_fake_mol()
+    assert fake.nbas == 1 and fake.bas_angular(0) == 0
+    assert fake.bas_exp(0)[0] == 0.0
+    assert abs(fake.bas_ctr_coeff(0)[0, 0] * 0.282094791773878143 - 1.) < 1e-15
+    mol = Mole(atom=geom.random_walk_molecule(8, seed=3),
+               basis='standin-6-31g*').build()
+    smol, coeff, counts = int3c.sort_mol(mol)
+    assert counts.sum() == smol.nbas
+    key = [(int(l), int(n)) for l, n in smol._bas[:, [1, 2]]]
+    off = np.append(0, np.cumsum(counts))
+    for g in range(len(counts)):
+        assert len(set(key[off[g]:off[g + 1]])) == 1
+    assert coeff.shape == (smol.nao_nr(cart=True), mol.nao)
