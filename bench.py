@@ -452,6 +452,9 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-int4c', action='store_true',
                     help='skip the ERI-tensor fill and density-fitting measurements')
+    ap.add_argument('--profile-fill', type=int, default=0,
+                    help='only run this many get_int4c calls of the (H2O)2 / '
+                         'cc-pVDZ ERI-tensor workload and exit (ncu target)')
     ap.add_argument('--profile-builds', type=int, default=0,
                     help='only run this many jk_build calls of the workload '
                          '(FP64, or mixed with --fp32-cutoff > 0 given '
@@ -495,6 +498,17 @@ def main():
     lib = jklib.load_library()
     if args.profile_builds > 0:
         return profile_builds(args, torch, lib)
+    if args.profile_fill > 0:
+        from byteqc_b200.cuobc.lib import int4c
+        from byteqc_b200.gto import Mole, geom
+        fmol = Mole(atom=geom.water_cluster(2, box=5.0, seed=0),
+                    basis='standin-cc-pvdz').build()
+        fopt = hf._VHFOpt(fmol).build(diag_block_with_triu=True)
+        for _ in range(args.profile_fill):
+            int4c.get_int4c(fmol, vhfopt=fopt)
+        torch.cuda.synchronize()
+        print('profile fill done: %d x (H2O)2 / cc-pVDZ' % args.profile_fill)
+        return
     mol, dm = make_workload(args.workload)
     t = time.perf_counter()
     opt = hf._VHFOpt(mol).build()
