@@ -139,3 +139,32 @@ def test_df_basis_helpers():
     for g in range(len(counts)):
         assert len(set(key[off[g]:off[g + 1]])) == 1
     assert coeff.shape == (smol.nao_nr(cart=True), mol.nao)
+
+
+def test_bins_and_group_split_match_oracle():
+    """The host bin offsets and (l, nprim) group capping of the product path
+    against the oracle's restatements of the same reference functions
+    (cuobc/scf/hf.py:567-578, 581-606), and the bin invariants the
+    class-pair entries rely on (monotone, starting at 0, covering the pairs
+    above the cutoff)."""
+    from byteqc_b200.cuobc.scf import hf
+    from oracle import hf_oracle
+    rng = np.random.default_rng(2)
+    for n in (1, 7, 300):
+        lq = np.sort(np.log(rng.uniform(1e-12, 1., n)))[::-1]
+        lq[lq > 0] = 0
+        for nbins in (1, 4, 10):
+            for cut in (1e-13, 1e-10):
+                a = hf._make_s_index_offsets(lq, nbins, cut)
+                b = hf_oracle.make_s_index_offsets(lq, nbins, cut)
+                assert np.array_equal(a, b)
+                assert a[0] == 0 and a[-1] <= n and np.all(np.diff(a) >= 0)
+                # every pair above the cutoff falls in a bin
+                assert a[-1] >= np.count_nonzero(lq >= np.log(cut))
+    uniq = np.array([[0, 3], [1, 1], [2, 1]])
+    counts = np.array([40, 25, 7])
+    for gs in (8, 30, 100):
+        x = hf._split_l_ctr_groups(uniq, counts, gs)
+        y = hf_oracle._split_l_ctr_groups(uniq, counts, gs)
+        assert np.array_equal(x[0], y[0]) and np.array_equal(x[1], y[1])
+        assert x[1].sum() == counts.sum()
