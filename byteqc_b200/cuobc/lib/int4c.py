@@ -67,9 +67,12 @@ def get_int4c_slice(cp_ij_id, cp_kl_id, vhfopt, buf=None, nbins=1):
     return (slice(i0, i1), slice(j0, j1), slice(k0, k1), slice(l0, l1), blk)
 
 
-def get_int4c(mol, blksize=None, vhfopt=None, nbins=1):
+def get_int4c(mol, blksize=None, vhfopt=None, batch=1, buf_size=0, nbins=1):
     """The (nao, nao, nao, nao) tensor (ij|kl) of the working basis as a
-    float64 CUDA tensor (cuobc/lib/int4c.py:44-70)."""
+    float64 CUDA tensor (cuobc/lib/int4c.py:44-70).  ``batch`` (the
+    reference's multi-GPU task batching) and ``buf_size`` (a staging-buffer
+    size of its basis set-up) are accepted for call compatibility; one GPU
+    per process fills the whole tensor."""
     from byteqc_b200.cuobc.scf.hf import _torch
     torch = _torch()
     vhfopt = _opt(mol, blksize, vhfopt)
