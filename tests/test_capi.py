@@ -34,6 +34,16 @@ def test_invalid_arguments_return_status():
     assert b'invalid' in lib.jk_last_error()
     s = np.zeros(2)
     assert lib.jk_rys_roots_host(0, 1.0, s.ctypes.data, s.ctypes.data) == 3
+    # the per-class-pair entries check their arguments before any CUDA call
+    bins = np.zeros(2, dtype=np.int32)
+    st = np.ones(4, dtype=np.int32)
+    assert lib.jk_fill_int2e(None, None, 0, st.ctypes.data, st.ctypes.data,
+                             bins.ctypes.data, bins.ctypes.data, 1, 0, 0,
+                             None) == 3
+    assert b'invalid' in lib.jk_last_error()
+    assert lib.jk_build_class_pair(None, None, None, None, 0, 1,
+                                   bins.ctypes.data, bins.ctypes.data, 1, 0,
+                                   0, None) == 3
 
 
 def test_product_tables_match_oracle_tables():
