@@ -41,7 +41,11 @@ WORKLOADS = {
 }
 
 
-def make_workload(name):
+def make_workload(name, oracle_overlap=False):
+    """Molecule and density of a named workload.  ``oracle_overlap`` takes
+    the overlap matrix for the density from the oracle's own integrals
+    instead of the engine's one-electron code (the reference arm maps no
+    engine library); the two agree to 1e-13."""
     from byteqc_b200.gto import Mole, geom
     nw, box, seed, basis = WORKLOADS[name]
     if nw == 'walk':
@@ -50,7 +54,11 @@ def make_workload(name):
     else:
         mol = Mole(atom=geom.water_cluster(nw, box=box, seed=seed),
                    basis=basis).build()
-    s = mol.intor('int1e_ovlp')
+    if oracle_overlap:
+        from oracle import gto_oracle
+        s = gto_oracle.overlap(mol)
+    else:
+        s = mol.intor('int1e_ovlp')
     dm = geom.scf_like_density(s, nocc=mol.nelectron // 2, seed=1)
     return mol, dm
 
@@ -388,13 +396,17 @@ def cpu_baseline(mol, dm, target_s=15.0, opt=None, repeats=1):
 
 
 def run_reference(args):
-    """The reference arm: the oracle (a port of the reference's CPU algorithm
-    for this path) on all host cores, rank 0 only; every step is one bounded
-    sample of the build, scaled by quartet count."""
+    """The reference arm, rank 0 only.  ``value``: the oracle (a port of the
+    reference's algorithm for this path; the reference has no CPU J/K of its
+    own) on all host cores, every step one bounded sample of the build
+    scaled by quartet count.  ``reference_gpu``: the reference's own kernels
+    (cuobc gint/gvhf compiled unmodified for sm_100a into oracle/_ref)
+    through its GINTbuild_jk task loop on the same workload and GPU, in a
+    child process.  No engine library is loaded on this arm."""
     rank = int(os.environ.get('RANK', '0'))
     if rank != 0:
         return
-    mol, dm = make_workload(args.workload)
+    mol, dm = make_workload(args.workload, oracle_overlap=True)
     vals, info = cpu_baseline(mol, dm, target_s=args.ref_sample_s,
                               repeats=args.warmup + args.steps)
     vals = vals if isinstance(vals, list) else [vals]
@@ -414,7 +426,31 @@ def run_reference(args):
         'e2e': {'value': value, 'unit': 'builds/s', 'h2d_bytes_per_step': 0,
                 'd2h_bytes_per_step': 0},
     }
+    if not args.no_reference_gpu:
+        line['reference_gpu'] = reference_gpu(args, mol, dm)
     print(json.dumps(line))
+
+
+def reference_gpu(args, mol, dm):
+    """The reference's own J/K kernels on this GPU (same workload, FP64):
+    CUDA events around its whole GINTbuild_jk task loop, density already on
+    the device, task bins precomputed; no L2 flush between builds."""
+    from oracle import ref_jk
+    if not ref_jk.available():
+        return {'unavailable': 'oracle/_ref not built (the reference sources '
+                               'were absent at build time)'}
+    reps = max(1, min(args.steps, 5))
+    try:
+        _, _, info = ref_jk.run('get_jk', mol, dm, timing=(2, reps))
+    except Exception as e:  # reported, not fatal: the CPU arm stands
+        return {'unavailable': str(e)[-300:]}
+    ms = info['ms_per_build']
+    return {'ms_per_build': ms, 'builds_per_s': 1e3 / ms, 'builds_timed': reps,
+            'class_pair_calls': info['launch_calls'], 'nbins': info['nbins'],
+            'what': 'ByteQC cuobc gint/gvhf kernels compiled unmodified for '
+                    'sm_100a (oracle/ref/Makefile), GINTbuild_jk per class '
+                    'pair as cuobc/scf/hf.py:get_jk calls it; AO transforms '
+                    'not included'}
 
 
 def profile_builds(args, torch, lib):
@@ -459,7 +495,9 @@ def main():
                     help='only run this many jk_build calls of the workload '
                          '(FP64, or mixed with --fp32-cutoff > 0 given '
                          'explicitly) and exit: the command profiled by ncu')
-    ap.add_argument('--ref-sample-s', type=float, default=8.0)
+    ap.add_argument('--ref-sample-s', type=float, default=4.0)
+    ap.add_argument('--no-reference-gpu', action='store_true',
+                    help='reference arm: skip timing the reference kernels')
     ap.add_argument('--batch-mols', type=int, default=256,
                     help='molecules of the batched workload (0: skip)')
     ap.add_argument('--batch-steps', type=int, default=1,

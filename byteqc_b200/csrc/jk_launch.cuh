@@ -1,7 +1,24 @@
 // Launchers of the J/K kernels, one per (li, lj, lk, ll) class and arithmetic
 // type, collected in a table indexed by JK_CLASS_INDEX(li, lj, lk, ll).
 #pragma once
+#include <atomic>
+
 #include "jk_kernels.cuh"
+
+// cudaFuncSetAttribute acts on the current device only, so the "already set"
+// flag of a kernel is kept per device (bit d of `done` for device d < 64;
+// devices beyond that set the attribute on every launch).
+template <class K>
+cudaError_t jk_smem_attr(K kernel, size_t smem, std::atomic<unsigned long long>& done) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+    if (bit && (done.load(std::memory_order_relaxed) & bit)) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_relaxed);
+    return e;
+}
 
 
 // One class quartet (one segment): the segment descriptor goes by value into
@@ -12,13 +29,8 @@ cudaError_t jk_launch(const JKSeg& seg, const long long* task0, long long max_ta
     if (max_tasks <= 0) return cudaSuccess;
     if constexpr (C::P == 0) {
         constexpr size_t smem = RysS<C::NROOTS>::WORDS * sizeof(double);
-        static bool attr_set = false;
-        if (!attr_set) {
-            cudaError_t e = cudaFuncSetAttribute(jk_thread_kernel<C, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem);
-            if (e != cudaSuccess) return e;
-            attr_set = true;
-        }
+        static std::atomic<unsigned long long> attr_done{0};
+        if (cudaError_t e = jk_smem_attr(jk_thread_kernel<C, R>, smem, attr_done); e != cudaSuccess) return e;
         long long want = (max_tasks + 127) / 128;
         long long cap = (long long)nsm * 16;
         int blocks = (int)(want < cap ? want : cap);
@@ -26,13 +38,8 @@ cudaError_t jk_launch(const JKSeg& seg, const long long* task0, long long max_ta
     } else {
         using S = JKTeamShape<C>;
         constexpr size_t smem = jk_team_smem<C, R>();
-        static bool attr_set = false;
-        if (!attr_set) {
-            cudaError_t e = cudaFuncSetAttribute(jk_team_kernel<C, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem);
-            if (e != cudaSuccess) return e;
-            attr_set = true;
-        }
+        static std::atomic<unsigned long long> attr_done{0};
+        if (cudaError_t e = jk_smem_attr(jk_team_kernel<C, R>, smem, attr_done); e != cudaSuccess) return e;
         long long want = (max_tasks + S::QPB - 1) / S::QPB;
         long long cap = (long long)nsm * 8;
         int blocks = (int)(want < cap ? want : cap);
@@ -51,13 +58,8 @@ cudaError_t jk_launch_batch(const JKSeg* segs, const long long* segt, int nseg, 
     if (max_tasks <= 0 || nseg <= 0) return cudaSuccess;
     if constexpr (C::P == 0) {
         constexpr size_t smem = RysS<C::NROOTS>::WORDS * sizeof(double);
-        static bool attr_set = false;
-        if (!attr_set) {
-            cudaError_t e = cudaFuncSetAttribute(jk_thread_kernel_batch<C, R>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return e;
-            attr_set = true;
-        }
+        static std::atomic<unsigned long long> attr_done{0};
+        if (cudaError_t e = jk_smem_attr(jk_thread_kernel_batch<C, R>, smem, attr_done); e != cudaSuccess) return e;
         long long want = (max_tasks + 127) / 128;
         long long cap = (long long)nsm * 16;
         int blocks = (int)(want < cap ? want : cap);
@@ -65,13 +67,8 @@ cudaError_t jk_launch_batch(const JKSeg* segs, const long long* segt, int nseg, 
     } else {
         using S = JKTeamShape<C>;
         constexpr size_t smem = jk_team_smem<C, R>();
-        static bool attr_set = false;
-        if (!attr_set) {
-            cudaError_t e = cudaFuncSetAttribute(jk_team_kernel_batch<C, R>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return e;
-            attr_set = true;
-        }
+        static std::atomic<unsigned long long> attr_done{0};
+        if (cudaError_t e = jk_smem_attr(jk_team_kernel_batch<C, R>, smem, attr_done); e != cudaSuccess) return e;
         long long want = (max_tasks + S::QPB - 1) / S::QPB;
         long long cap = (long long)nsm * 8;
         int blocks = (int)(want < cap ? want : cap);

@@ -10,17 +10,25 @@
 // allocates its row-offset and segment buffers on first use and grows them
 // when a larger class pair comes; this entry point never does.
 //
-// How: the scratch (row offsets, task counts and the bins) lives in the file-scope array jk_na_scratch below, sized for at
-// most JK_NA_MAX_ROWS shell pairs in the ij class and JK_NA_MAX_BINS bins.
-// Every GPU that loads libjk.so holds this array (about 1 MB) until the
-// process exits.  Host code cannot use the array's name as a device address
-// (in host code it names a host-side stand-in), so the first call on each
-// device looks the address up with cudaGetSymbolAddress, with that device
-// current, and caches it; that first call should come before any stream
-// capture.  All calls share the one array and the previous call's contents
-// stay in it: every field a call reads is rewritten by that call before use.
-// Calls whose GPU work overlaps (on different streams, or from different
-// threads) race on the array and must be serialised by the caller.
+// How: the scratch (row offsets, task counts and the bins) lives in the
+// file-scope array jk_na_scratch below, sized for at most JK_NA_MAX_ROWS
+// shell pairs in the ij class and JK_NA_MAX_BINS bins.  Every GPU that loads
+// this module holds the array (about 1 MB) until the process exits.  Host
+// code cannot use the array's name as a device address (in host code it
+// names a host-side stand-in), so the first call on each device looks the
+// address up with cudaGetSymbolAddress, with that device current, and caches
+// it; that first call should come before any stream capture.  With CUDA's
+// lazy module loading (the default) the array is placed on a device only at
+// that lookup, so a caller whose pool reserves most of the device's memory
+// should make the first call (a call with vj = vk = NULL does only the
+// lookup) before the reservation, or run with CUDA_MODULE_LOADING=EAGER.
+// The cached address is not valid after cudaDeviceReset.  All calls share
+// the one array and the previous call's contents stay in it: every field a
+// call reads is rewritten by that call before use.  Calls whose GPU work
+// overlaps (on different streams, or from different threads) race on the
+// array and must be serialised by the caller.  Like jk_build_class_pair, the
+// call returns after its GPU work has finished (it synchronises the stream),
+// so the host bins and the outputs are free to use on return.
 #include <mutex>
 
 #include "jk_internal.h"
@@ -59,9 +67,12 @@ static int na_scratch(unsigned char** out) {
 // Row offsets of one class pair from the reference's host bins
 // (cuobc/lib/gvhf/nr_jk_driver.cu:252-280): row ij in bin s keeps
 // kl < bins_kl[nbins - s]; a diagonal class pair keeps kl <= ij.
-// One block; writes qoff[0..n_ij] and task0 = {0, total}.
+// One block; writes qoff[0..n_ij] and task0 = {0, total}.  A count is
+// clamped to the n_kl pairs of the kl class, so bins beyond the class cannot
+// take the task total past the launch bound.
 __global__ void jk_na_qoff_kernel(const int* __restrict__ bins_ij, const int* __restrict__ bins_kl, int nbins,
-                                  int n_ij, int diag, long long* __restrict__ qoff, long long* __restrict__ task0) {
+                                  int n_ij, int n_kl, int diag, long long* __restrict__ qoff,
+                                  long long* __restrict__ task0) {
     __shared__ long long carry;
     __shared__ long long wsum[32];
     if (threadIdx.x == 0) {
@@ -80,6 +91,8 @@ __global__ void jk_na_qoff_kernel(const int* __restrict__ bins_ij, const int* __
             }
             if (lo < nbins) {
                 cnt = bins_kl[nbins - lo];
+                if (cnt > n_kl) cnt = n_kl;
+                if (cnt < 0) cnt = 0;
                 if (diag && cnt > ij + 1) cnt = ij + 1;
             }
         }
@@ -127,26 +140,29 @@ extern "C" int jk_build_class_pair_noalloc(jk_basis_t* b, double* vj, double* vk
         return jk_internal_set_err(JK_ERR_ARG,
                                    "jk_build_class_pair_noalloc: the ij class has more than 131072 shell pairs; "
                                    "use jk_build_class_pair");
-    if (!vj && !vk) return JK_OK;
     unsigned char* sc;
     rc = na_scratch(&sc);
     if (rc) return rc;
+    if (!vj && !vk) return JK_OK;
     cudaStream_t st = (cudaStream_t)stream;
     long long* d_task0 = (long long*)(sc + JK_NA_OFF_TASK0);
     int* d_bins_ij = (int*)(sc + JK_NA_OFF_BINS);
     int* d_bins_kl = d_bins_ij + (nbins + 1);
     long long* d_qoff = (long long*)(sc + JK_NA_OFF_QOFF);
-    // the host bins are staged by the copy engine from pageable memory: the
-    // copies return once the host data has been taken
     cudaError_t e = cudaMemcpyAsync(d_bins_ij, bins_locs_ij, sizeof(int) * (nbins + 1), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(d_bins_kl, bins_locs_kl, sizeof(int) * (nbins + 1), cudaMemcpyHostToDevice, st);
     JKSeg seg;
     jk_internal_fill_seg(b, cp_ij, cp_kl, d_qoff, n_ij, dm, n_dm, vj, vk, &seg);
     if (e != cudaSuccess) return jk_internal_set_err(JK_ERR_CUDA, cudaGetErrorString(e));
-    jk_na_qoff_kernel<<<1, 1024, 0, st>>>(d_bins_ij, d_bins_kl, nbins, n_ij, cp_ij == cp_kl, d_qoff, d_task0);
+    jk_na_qoff_kernel<<<1, 1024, 0, st>>>(d_bins_ij, d_bins_kl, nbins, n_ij, n_kl, cp_ij == cp_kl, d_qoff, d_task0);
     e = cudaGetLastError();
     if (e != cudaSuccess) return jk_internal_set_err(JK_ERR_CUDA, cudaGetErrorString(e));
     long long max_tasks = cp_ij == cp_kl ? (long long)n_ij * (n_ij + 1) / 2 : (long long)n_ij * n_kl;
-    return jk_internal_launch(b, cp_ij, cp_kl, seg, d_task0, max_tasks, stream);
+    rc = jk_internal_launch(b, cp_ij, cp_kl, seg, d_task0, max_tasks, stream);
+    if (rc) return rc;
+    // same synchronous contract as jk_build_class_pair
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return jk_internal_set_err(JK_ERR_CUDA, cudaGetErrorString(e));
+    return JK_OK;
 }

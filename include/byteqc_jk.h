@@ -106,8 +106,14 @@ int jk_fill_int2e(jk_basis_t *basis, double *eri, int nao, const int *strides, c
  * reference.  It allocates nothing: its scratch is a fixed device array of
  * about 1 MB inside libjk.so, held on every GPU that loads the library.
  * Limits: at most 131072 shell pairs in the ij class and nbins <= 1024;
- * larger requests return JK_ERR_ARG.  The first call on a device looks up the
- * array's device address (make it before any stream capture).  All calls
+ * larger requests return JK_ERR_ARG.  The bins must be non-decreasing with
+ * bins_locs_kl[nbins] <= the kl class's pair count (larger counts are
+ * clamped to it).  The first call on a device looks up the array's device
+ * address (make it before any stream capture); with CUDA's lazy module
+ * loading that lookup is also when the array is placed on the device, so a
+ * caller whose pool reserves most of the memory should make one call with
+ * vj = vk = NULL (which does only the lookup) before the reservation.  Like
+ * jk_build_class_pair it returns after the GPU work has finished.  All calls
  * share the array: calls whose GPU work overlaps race and must be serialised
  * by the caller.
  */

@@ -16,14 +16,17 @@ Follows, step by step:
     hf.py:567-578), the per-task kernel call, then J = 2 C^T (V + V^T) C and
     K = C^T (V + V^T) C.
 The Schwarz matrix is the oracle's own (C, same definition as PySCF's
-CVHFsetnr_direct_scf).
+CVHFsetnr_direct_scf); the radial normalisation and the Cartesian-to-spherical
+transform are the oracle's own too (``gto_oracle``), so they do not share
+code with the product's ``byteqc_b200.gto``.
 """
 import ctypes
 
 import numpy as np
 
 import oracle
-from byteqc_b200.gto import mole as gmole
+from byteqc_b200.gto import mole as gmole  # libcint slot indices only
+from oracle import gto_oracle
 
 LMAX_ON_GPU = 5
 
@@ -54,7 +57,7 @@ def basis_seg_contraction(mol):
                 pcoeff = shell[gmole.PTR_COEFF]
                 pexp = shell[gmole.PTR_EXP]
                 exps = _env[pexp:pexp + nprim]
-                norm = gmole.gto_norm(l, exps)
+                norm = gto_oracle.gto_norm(l, exps)
                 c = _env[pcoeff:pcoeff + nprim * nctr].reshape(nctr, nprim)
                 c = np.einsum('ip,p,ef->iepf', c, 1 / norm, np.eye(nf))
                 coeff.append(c.reshape(nf * nctr, nf * nprim).T)
@@ -83,7 +86,7 @@ def basis_seg_contraction(mol):
             r += c.shape[0]
             cc += c.shape[1]
         return pmol, out
-    c2s = mol.cart2sph_coeff()
+    c2s = gto_oracle.cart2sph_coeff(mol)
     cols = np.cumsum([0] + [c.shape[0] for c in contr_coeff])
     rows = np.cumsum([0] + [c.shape[1] for c in contr_coeff])
     out = np.empty((cols[-1], c2s.shape[1]))

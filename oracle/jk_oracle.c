@@ -388,3 +388,94 @@ long oracle_build_jk(const int *atm, const int *bas, const double *env, int nbas
     }
     return count;
 }
+
+/* ---- overlap ---------------------------------------------------------- */
+/* Cartesian overlap <i|j> of a basis whose shells carry one contraction
+ * each (the decontracted working basis), in libcint's conventions: the
+ * env coefficients hold the radial normalisation, the s and p common
+ * factors are applied at evaluation time (as for the ERIs above).  1D
+ * overlaps by the Obara-Saika recursion on the Gaussian product centre,
+ * S(a+1,0) = PA S(a,0) + a/(2g) S(a-1,0), then S(a,b+1) = S(a+1,b) + AB S(a,b).
+ * Used to build test densities and to check the normalisation of the
+ * contracted spherical basis without the product library.  Returns 1 for a
+ * shell with more than one contraction or l > LMAX. */
+int oracle_ovlp_cart(const int *atm, const int *bas, const double *env, int nbas, const int *ao_loc,
+                     double *out) {
+    basis_t b = {atm, bas, env, nbas};
+    int nao = ao_loc[nbas];
+    for (int s = 0; s < nbas; s++)
+        if (bas[s * BAS_SLOTS + 3] != 1 || bas[s * BAS_SLOTS + ANG_OF] > LMAX) return 1;
+#pragma omp parallel for schedule(dynamic)
+    for (int ish = 0; ish < nbas; ish++) {
+        for (int jsh = 0; jsh < nbas; jsh++) {
+            int li = bas[ish * BAS_SLOTS + ANG_OF], lj = bas[jsh * BAS_SLOTS + ANG_OF];
+            int npi = bas[ish * BAS_SLOTS + NPRIM_OF], npj = bas[jsh * BAS_SLOTS + NPRIM_OF];
+            const double *ri = shell_center(&b, ish), *rj = shell_center(&b, jsh);
+            const double *ei = env + bas[ish * BAS_SLOTS + PTR_EXP], *ej = env + bas[jsh * BAS_SLOTS + PTR_EXP];
+            const double *ci = env + bas[ish * BAS_SLOTS + PTR_COEFF], *cj = env + bas[jsh * BAS_SLOTS + PTR_COEFF];
+            int lxi[NF_MAX], lyi[NF_MAX], lzi[NF_MAX], lxj[NF_MAX], lyj[NF_MAX], lzj[NF_MAX];
+            cart_list(li, lxi, lyi, lzi);
+            cart_list(lj, lxj, lyj, lzj);
+            int nfi = ncart(li), nfj = ncart(lj);
+            double blk[NF_MAX * NF_MAX];
+            memset(blk, 0, sizeof(blk));
+            double r2 = 0;
+            for (int d = 0; d < 3; d++) r2 += (ri[d] - rj[d]) * (ri[d] - rj[d]);
+            for (int ip = 0; ip < npi; ip++)
+                for (int jp = 0; jp < npj; jp++) {
+                    double a = ei[ip], c = ej[jp], g = a + c;
+                    double pref = ci[ip] * cj[jp] * exp(-a * c / g * r2) * pow(M_PI / g, 1.5);
+                    double s1[3][2 * LMAX + 2][LMAX + 1];
+                    for (int d = 0; d < 3; d++) {
+                        double P = (a * ri[d] + c * rj[d]) / g;
+                        double PA = P - ri[d], AB = ri[d] - rj[d];
+                        double t[2 * LMAX + 2][LMAX + 1];
+                        t[0][0] = 1.;
+                        for (int x = 0; x < li + lj; x++)
+                            t[x + 1][0] = PA * t[x][0] + (x > 0 ? x / (2 * g) * t[x - 1][0] : 0.);
+                        for (int y = 0; y < lj; y++)
+                            for (int x = 0; x + y + 1 <= li + lj; x++) t[x][y + 1] = t[x + 1][y] + AB * t[x][y];
+                        for (int x = 0; x <= li; x++)
+                            for (int y = 0; y <= lj; y++) s1[d][x][y] = t[x][y];
+                    }
+                    for (int i = 0; i < nfi; i++)
+                        for (int j = 0; j < nfj; j++)
+                            blk[i * nfj + j] += pref * s1[0][lxi[i]][lxj[j]] * s1[1][lyi[i]][lyj[j]] *
+                                                s1[2][lzi[i]][lzj[j]];
+                }
+            double f = common_fac_sp(li) * common_fac_sp(lj);
+            for (int i = 0; i < nfi; i++)
+                for (int j = 0; j < nfj; j++)
+                    out[(size_t)(ao_loc[ish] + i) * nao + ao_loc[jsh] + j] = f * blk[i * nfj + j];
+        }
+    }
+    return 0;
+}
+
+/* The primitive-pair table of a pair list in the reference's cache layout
+ * (a12 | e12 | x12 | y12 | z12, each n_prim_pairs long, pairs in list order,
+ * primitives bra-major; pair_data.c:83-141), from prim_pair above.  Lets the
+ * tests compare the oracle's pair data with the reference's own
+ * GINTinit_aexyz. */
+long oracle_pair_data(const int *atm, const int *bas, const double *env, int nbas, const int *pair2bra,
+                      const int *pair2ket, int npairs, double diag_fac, double *out, long cap) {
+    basis_t b = {atm, bas, env, nbas};
+    long n = 0;
+    for (int p = 0; p < npairs; p++)
+        n += (long)bas[pair2bra[p] * BAS_SLOTS + NPRIM_OF] * bas[pair2ket[p] * BAS_SLOTS + NPRIM_OF];
+    if (n > cap) return -n;
+    long c = 0;
+    for (int p = 0; p < npairs; p++) {
+        int ish = pair2bra[p], jsh = pair2ket[p];
+        int npi = bas[ish * BAS_SLOTS + NPRIM_OF], npj = bas[jsh * BAS_SLOTS + NPRIM_OF];
+        for (int ip = 0; ip < npi; ip++)
+            for (int jp = 0; jp < npj; jp++, c++) {
+                double P[3];
+                prim_pair(&b, ish, jsh, ip, jp, diag_fac, out + c, out + n + c, P);
+                out[2 * n + c] = P[0];
+                out[3 * n + c] = P[1];
+                out[4 * n + c] = P[2];
+            }
+    }
+    return n;
+}

@@ -271,3 +271,86 @@ def test_oracle_reproduces_golden(case):
     vj, vk = hf_oracle.get_jk(mol, dm)
     np.testing.assert_allclose(vj, g[case + '/vj'], rtol=0, atol=1e-12)
     np.testing.assert_allclose(vk, g[case + '/vk'], rtol=0, atol=1e-12)
+
+
+def test_basis_conventions_independent_of_product():
+    """The oracle's radial normalisation and Cartesian-to-spherical matrix
+    (oracle/gto_oracle.py: scipy's gamma function and spherical harmonics)
+    against the product's (byteqc_b200.gto.mole: closed-form solid
+    harmonics) for l = 0..5; the two are derived independently, so a wrong
+    matrix or norm cannot cancel between the engine and the oracle."""
+    from byteqc_b200.gto import mole
+    from oracle import gto_oracle
+    for l in range(6):
+        np.testing.assert_allclose(gto_oracle.cart2sph(l), mole.cart2sph(l),
+                                   rtol=0, atol=5e-14)
+        e = np.array([0.07, 0.9, 13.0, 4000.0])
+        np.testing.assert_allclose(gto_oracle.gto_norm(l, e),
+                                   mole.gto_norm(l, e), rtol=1e-14)
+
+
+@pytest.mark.parametrize('basis', ['standin-cc-pvdz', 'standin-def2-tzvp',
+                                   'standin-6-31g*'])
+def test_contracted_spherical_overlap_is_normalised(basis):
+    """Every contracted spherical function has unit norm under the oracle's
+    own overlap integrals (Obara-Saika, jk_oracle.c) and transforms, and the
+    overlap matrix equals the product's one-electron code."""
+    from oracle import gto_oracle
+    mol = Mole(atom=geom.water_cluster(2, box=5.0, seed=0),
+               basis=basis).build()
+    s = gto_oracle.overlap(mol)
+    assert abs(np.diag(s) - 1).max() < 1e-13
+    np.testing.assert_allclose(s, mol.intor('int1e_ovlp'), rtol=0, atol=1e-13)
+
+
+@pytest.mark.parametrize('basis', ['standin-cc-pvdz', 'standin-def2-tzvp',
+                                   'standin-6-31g*'])
+def test_pair_data_matches_reference_cache(basis):
+    """The oracle's primitive-pair table (a12, e12, product centres, the
+    0.5 diagonal factor) is identical, bit for bit, to the one the
+    reference's own GINTinit_basis_prod_cpu (cuobc/lib/gint/pair_data.c,
+    compiled unmodified into oracle/_ref/) builds from the same pair lists;
+    host code only, no GPU."""
+    import ctypes
+    import oracle
+    from oracle import hf_oracle, ref_jk
+    if not ref_jk.available():
+        pytest.skip('oracle/_ref not built (needs the reference sources)')
+    gint, _ = ref_jk.libs()
+    mol = Mole(atom=geom.water_cluster(3, box=6.0, seed=2),
+               basis=basis).build()
+    for triu in (False, True):
+        opt = hf_oracle.VHFOpt(mol).build(diag_block_with_triu=triu)
+        pmol = opt.mol
+        atm = np.ascontiguousarray(pmol._atm, dtype=np.int32)
+        bas = np.ascontiguousarray(pmol._bas, dtype=np.int32)
+        env = np.ascontiguousarray(pmol._env)
+        p2s = np.ascontiguousarray(opt.bas_pair2shls, dtype=np.int32)
+        locs = np.ascontiguousarray(opt.bas_pairs_locs, dtype=np.int32)
+        ncp = len(opt.log_qs)
+        coords = np.empty(pmol.nbas * 3)
+        cache = ctypes.POINTER(ref_jk.BasisProdCache)()
+        P = ref_jk._ptr
+        gint.GINTinit_basis_prod_cpu(
+            ctypes.byref(cache), ctypes.c_double(opt.diag_fac), P(coords),
+            P(p2s), P(locs), ctypes.c_int(ncp), P(atm),
+            ctypes.c_int(pmol.natm), P(bas), ctypes.c_int(pmol.nbas), P(env))
+        c = cache.contents
+        n = c.primitive_pairs_locs[ncp]
+        ref = np.ctypeslib.as_array(c.aexyz, (n * 5,)).copy()
+        for k in range(ncp):
+            t = c.cptype[k]
+            i, j = p2s[0, locs[k]], p2s[1, locs[k]]
+            assert (t.l_bra, t.l_ket) == (pmol._bas[i, 1], pmol._bas[j, 1])
+            assert t.npairs == locs[k + 1] - locs[k]
+        mine = np.zeros(n * 5)
+        lib = oracle.lib()
+        lib.oracle_pair_data.restype = ctypes.c_long
+        got = lib.oracle_pair_data(
+            P(atm), P(bas), P(env), ctypes.c_int(pmol.nbas),
+            P(np.ascontiguousarray(p2s[0])), P(np.ascontiguousarray(p2s[1])),
+            ctypes.c_int(p2s.shape[1]), ctypes.c_double(opt.diag_fac),
+            P(mine), ctypes.c_long(n * 5))
+        assert got == n
+        np.testing.assert_array_equal(mine, ref)
+        gint.GINTdel_basis_prod(ctypes.byref(cache))
