@@ -82,8 +82,11 @@ def batch_workload(nmol=256, seed=4, basis='standin-6-31g*'):
 def bench_batch(args, torch, timed):
     """Builds of the 256-molecule workload: per-molecule launches in FP64 (the
     plain engine), and the batch (one launch per shared class) replayed from a
-    captured CUDA graph in FP64 and in mixed precision.  Returns the 'batch'
-    sub-object of the bench line."""
+    captured CUDA graph in FP64 and in mixed precision, first with static
+    chunks, then with the launch shapes the autotuner picks; then an RHF of
+    every molecule through the batched server, FP64 and mixed, and the
+    energy difference of each.  Returns the 'batch' sub-object of the bench
+    line."""
     from byteqc_b200.cuobc.scf import hf
     from byteqc_b200.cuobc.scf.batch import JKBatch
     mols, dms = batch_workload(args.batch_mols)
@@ -111,23 +114,74 @@ def bench_batch(args, torch, timed):
     per_molecule()
     ms = timed(per_molecule, args.batch_steps)
     res['per_molecule_fp64'] = {'ms': ms, 'builds_per_s': len(mols) * 1e3 / ms}
-    for name, cut in (('graph_fp64', 0.), ('graph_mixed', args.fp32_cutoff)):
-        batch.capture(d_dms, fp32_cutoff=cut)
-        g = batch._graph[0]
-        g.replay()
-        ms = timed(g.replay, args.batch_steps)
-        res[name] = {'ms': ms, 'builds_per_s': len(mols) * 1e3 / ms,
-                     'max_abs_err_jk_vs_fp64': err_vs_ref()}
+
+    def graphs(suffix):
+        for name, cut in (('graph_fp64', 0.), ('graph_mixed', args.fp32_cutoff)):
+            batch.capture(d_dms, fp32_cutoff=cut)
+            g = batch._graph[0]
+            g.replay()
+            ms = timed(g.replay, args.batch_steps)
+            res[name + suffix] = {'ms': ms, 'builds_per_s': len(mols) * 1e3 / ms,
+                                  'max_abs_err_jk_vs_fp64': err_vs_ref()}
+    graphs('')
+    t = time.perf_counter()
+    info = batch.tune(d_dms, fp32_cutoff=args.fp32_cutoff)
+    tune_s = time.perf_counter() - t
+    batch._load(d_dms)
+    graphs('_tuned')
     res['graph_mixed']['fp32_cutoff'] = args.fp32_cutoff
+    res['graph_mixed_tuned']['fp32_cutoff'] = args.fp32_cutoff
     base = res['per_molecule_fp64']['builds_per_s']
+    shapes = {'launches': len(info),
+              'persistent_fp64': sum(1 for k in info if k['fp64']['grab'] > 0),
+              'persistent_fp32': sum(1 for k in info if k['fp32']['grab'] > 0),
+              'tune_s': tune_s}
     batch.close()
-    return {'molecules': len(mols), 'basis': 'standin-6-31g*',
-            'nbf_min': min(nbf), 'nbf_max': max(nbf), 'nbf_mean': float(np.mean(nbf)),
-            'setup_s': setup, 'variants': res,
-            'speedup_graph_mixed_vs_per_molecule_fp64':
-                res['graph_mixed']['builds_per_s'] / base,
-            'speedup_graph_mixed_vs_graph_fp64':
-                res['graph_mixed']['builds_per_s'] / res['graph_fp64']['builds_per_s']}
+    out = {'molecules': len(mols), 'basis': 'standin-6-31g*',
+           'nbf_min': min(nbf), 'nbf_max': max(nbf), 'nbf_mean': float(np.mean(nbf)),
+           'setup_s': setup, 'variants': res, 'tuned_shapes': shapes,
+           'speedup_graph_mixed_tuned_vs_per_molecule_fp64':
+               res['graph_mixed_tuned']['builds_per_s'] / base,
+           'speedup_graph_fp64_tuned_vs_per_molecule_fp64':
+               res['graph_fp64_tuned']['builds_per_s'] / base,
+           'speedup_graph_mixed_vs_graph_fp64':
+               res['graph_mixed']['builds_per_s'] / res['graph_fp64']['builds_per_s']}
+    if args.batch_scf > 0:
+        out['scf'] = bench_batch_scf(args, mols[:args.batch_scf])
+    return out
+
+
+def bench_batch_scf(args, mols):
+    """RHF of every molecule of the batched workload through the batched
+    server (all requests admitted at once, one batched J/K pass per
+    iteration, converged when the energy changes by less than 1e-9 Eh), in
+    FP64 and in mixed precision: the energy difference of every molecule."""
+    from byteqc_b200.cuobc.scf.serve import JKServer
+    res = {}
+    for name, cut in (('fp64', None), ('mixed', args.fp32_cutoff)):
+        t = time.perf_counter()
+        srv = JKServer(n_iter=args.batch_scf_iters, conv_tol=1e-9,
+                       fp32_cutoff=cut, max_slots=len(mols),
+                       hbm_budget_bytes=150 << 30)
+        for m in mols:
+            srv.submit(m)
+        srv.run_until_empty()
+        fin = sorted(srv.finished, key=lambda r: r.rid)
+        res[name] = {'wall_s': time.perf_counter() - t, 'steps': srv.steps,
+                     'energies': [r.energies[-1] for r in fin],
+                     'iterations': [len(r.energies) for r in fin],
+                     'converged': sum(1 for r in fin if r.converged)}
+    de = np.array(res['mixed']['energies']) - np.array(res['fp64']['energies'])
+    return {'molecules': len(mols), 'conv_tol': 1e-9,
+            'fp32_cutoff': args.fp32_cutoff,
+            'converged_fp64': res['fp64']['converged'],
+            'converged_mixed': res['mixed']['converged'],
+            'max_abs_de': float(np.abs(de).max()),
+            'mean_abs_de': float(np.abs(de).mean()),
+            'de_per_molecule': [float(x) for x in de],
+            'iterations_fp64_mean': float(np.mean(res['fp64']['iterations'])),
+            'iterations_mixed_mean': float(np.mean(res['mixed']['iterations'])),
+            'wall_s_fp64': res['fp64']['wall_s'], 'wall_s_mixed': res['mixed']['wall_s']}
 
 
 def bench_sweep(args, torch, timed):
@@ -164,6 +218,24 @@ def bench_sweep(args, torch, timed):
     opt.clear()
     return {'workload': 'h2o64-dz', 'nao': int(mol.nao), 'ms_per_build_fp64': ms64,
             'scf_fp64': scf64, 'rows': rows}
+
+
+def bench_rhf(args, mol, opt):
+    """Full RHF of the headline workload to |dE| < 1e-9 Eh (DIIS,
+    incremental Fock builds) in FP64, and in mixed precision at the bench's
+    FP32 cutoff: energies, cycles, J/K builds and wall time."""
+    from byteqc_b200.cuobc.scf import RHF
+    out = {'workload': args.workload, 'conv_tol': 1e-9}
+    for name, cut in (('fp64', None), ('mixed', args.fp32_cutoff or None)):
+        t = time.perf_counter()
+        mf = RHF(mol, fp32_cutoff=cut)
+        mf._opt_gpu = opt
+        e = mf.kernel()
+        out[name] = {'e_tot': e, 'converged': mf.converged, 'cycles': mf.cycles,
+                     'jk_builds': mf.jk_builds, 'wall_s': time.perf_counter() - t}
+    if out['mixed']['e_tot'] is not None:
+        out['de_mixed'] = out['mixed']['e_tot'] - out['fp64']['e_tot']
+    return out
 
 
 def serve_workload(nreq, seed=5, max_nbf=2000, min_nbf=50):
@@ -502,14 +574,21 @@ def main():
                     help='molecules of the batched workload (0: skip)')
     ap.add_argument('--batch-steps', type=int, default=1,
                     help='timed repetitions of each batched variant')
+    ap.add_argument('--batch-scf', type=int, default=256,
+                    help='molecules of the batched workload run to SCF '
+                         'convergence in FP64 and mixed (0: skip)')
+    ap.add_argument('--batch-scf-iters', type=int, default=40,
+                    help='iteration cap of those SCF runs')
+    ap.add_argument('--no-rhf', action='store_true',
+                    help='skip the full RHF of the headline workload')
     ap.add_argument('--no-sweep', action='store_true',
                     help='skip the mixed-precision cutoff sweep with SCF energies')
     ap.add_argument('--sweep-cutoffs', type=float, nargs='*',
                     default=[1e-8, 1e-7, 1e-6, 1e-5, 1e-4])
-    ap.add_argument('--serve-requests', type=int, default=16,
+    ap.add_argument('--serve-requests', type=int, default=48,
                     help='requests of the serving stream (0: skip)')
     ap.add_argument('--serve-iters', type=int, default=15)
-    ap.add_argument('--serve-max-nbf', type=int, default=600,
+    ap.add_argument('--serve-max-nbf', type=int, default=2000,
                     help='largest request in basis functions (2000 for the '
                          'full 50-2000 range)')
     ap.add_argument('--fp32-cutoff', type=float, default=1e-6,
@@ -694,6 +773,8 @@ def main():
                 'd2h_bytes_per_step': int(2 * dm.nbytes)},
         'clocks': clk.summary(),
     }
+    if not args.no_rhf and world == 1:
+        line['rhf'] = bench_rhf(args, mol, opt)
     if args.batch_mols > 0 and world == 1:
         line['batch'] = bench_batch(args, torch, timed)
     if not args.no_sweep and world == 1:

@@ -94,7 +94,7 @@ static void nuc_prim(int li, int lj, double a, double b, const double *A, const 
      * a straightforward recursion in a scratch array indexed by
      * (ia = cart index of total l_a <= L) only on the bra, then HRR. */
     /* VRR on the bra up to L, then horizontal transfer to j */
-    int nc = 0, cidx[11][11][11];
+    int nc = 0, cidx[13][13][13];
     for (int l = 0; l <= L; l++)
         for (int x = l; x >= 0; x--)
             for (int y = l - x; y >= 0; y--) cidx[x][y][l - x - y] = nc++;
@@ -170,7 +170,7 @@ int jk_int1e_cart(int which, const int *atm, int natm, const int *bas, int nbas,
     ao_loc[0] = 0;
     for (int i = 0; i < nbas; i++) {
         int l = bas[i * BAS_SLOTS + ANG_OF];
-        if (l > 5) { free(ao_loc); return 2; }
+        if (l > 6) { free(ao_loc); return 2; }
         ao_loc[i + 1] = ao_loc[i] + ncart(l) * bas[i * BAS_SLOTS + NCTR_OF];
     }
     int nao = ao_loc[nbas];

@@ -2,13 +2,23 @@
 //
 // The single-molecule path launches one kernel per class quartet; for small
 // molecules those launches are tiny and the GPU idles between them.  Here the
-// class quartets of all molecules that share a class key (the four angular
-// momenta and the two primitive counts) become segments of ONE launch, so a
-// batch of hundreds of molecules costs one launch per class key plus three
-// bookkeeping launches (density condensation, screening, segment prefixes),
-// all on one stream with no host synchronisation; the whole sequence can be
-// captured into a CUDA graph and replayed every SCF iteration.
+// class quartets of all molecules that share a class key become segments of
+// ONE launch, so a batch of hundreds of molecules costs one launch per class
+// key plus three bookkeeping launches (density condensation, screening,
+// segment prefixes), with no host synchronisation; the whole sequence can be
+// captured into a CUDA graph and replayed every SCF iteration.  A key is the
+// class (four angular momenta), plus the two primitive counts for the team
+// kernels, whose blocks loop over the primitives in step.  Within a key the
+// segments are ordered by descending task count, so the largest molecules'
+// work is handed out first.
+//
+// Launch shape per key (JKBatchCfg): static contiguous chunks, or the
+// persistent mode in which a grid of the device's resident capacity takes
+// chunks from a device counter.  jk_batch_tune times the candidate shapes of
+// every key on the batch itself and keeps the fastest; its choices can be
+// written to and read from a cache file.
 #include <math.h>
+#include <stdio.h>
 #include <string.h>
 
 #include <algorithm>
@@ -38,9 +48,12 @@ struct JKSym {
 };
 
 struct JKBatchKey {
-    int cls, np_ij, np_kl;
+    int cls, np_ij, np_kl;                  // np_* = -1: any primitive count
     std::vector<std::pair<int, int>> segs;  // (molecule, class quartet)
+    std::vector<long long> seg_tasks;       // unscreened tasks of each segment
     long long max_tasks = 0;
+    JKBatchCfg cfg[2] = {{nullptr, 0, 1}, {nullptr, 0, 1}};  // FP64 part, FP32 part (queue set at launch)
+    float tuned_ms[2] = {-1.f, -1.f};
 };
 
 struct jk_batch {
@@ -71,6 +84,7 @@ struct jk_batch {
     // captured graph
     cudaGraphExec_t graph = nullptr;
     JKFanout fan;  // side streams of the class launches
+    unsigned long long* d_queue = nullptr;  // 2 work counters per key (persistent launches)
     // pair-packed J side: every molecule's packed densities, then every
     // molecule's packed J accumulators (one memset clears them all)
     double* d_pk = nullptr;
@@ -151,6 +165,7 @@ static void free_batch(jk_batch* t) {
     cudaFree((void*)t->d_cnt64);
     cudaFree((void*)t->d_cnt32);
     cudaFree(t->d_key_off);
+    cudaFree(t->d_queue);
     cudaFree(t->d_work);
     cudaFree(t->d_sym);
     if (t->blas) cublasDestroy(t->blas);
@@ -176,6 +191,7 @@ static int batch_create(jk_basis_t* const* bases, int nmol, jk_batch* t) {
             int cls = jk_internal_class_index(b, cq.cp_ij, cq.cp_kl);
             int np_ij = b->h_group_nprim[cq.gi] * b->h_group_nprim[cq.gj];
             int np_kl = b->h_group_nprim[cq.gk] * b->h_group_nprim[cq.gl];
+            if (!jk_internal_class_team(cls)) np_ij = np_kl = -1;
             auto key = std::make_tuple(cls, np_ij, np_kl);
             auto it = kidx.find(key);
             if (it == kidx.end()) {
@@ -188,10 +204,26 @@ static int batch_create(jk_basis_t* const* bases, int nmol, jk_batch* t) {
                 it = kidx.find(key);
             }
             JKBatchKey& k = t->keys[it->second];
+            const long long n = cq.cp_ij == cq.cp_kl ? (long long)cq.n_ij * (cq.n_ij + 1) / 2
+                                                     : (long long)cq.n_ij * cq.n_kl;
             k.segs.push_back({m, c});
-            k.max_tasks += cq.cp_ij == cq.cp_kl ? (long long)cq.n_ij * (cq.n_ij + 1) / 2
-                                                : (long long)cq.n_ij * cq.n_kl;
+            k.seg_tasks.push_back(n);
+            k.max_tasks += n;
         }
+    }
+    // longest first within every key (stable: ties keep molecule order)
+    for (auto& k : t->keys) {
+        std::vector<int> ord(k.segs.size());
+        for (size_t i = 0; i < ord.size(); i++) ord[i] = (int)i;
+        std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return k.seg_tasks[a] > k.seg_tasks[b]; });
+        std::vector<std::pair<int, int>> segs(ord.size());
+        std::vector<long long> tasks(ord.size());
+        for (size_t i = 0; i < ord.size(); i++) {
+            segs[i] = k.segs[ord[i]];
+            tasks[i] = k.seg_tasks[ord[i]];
+        }
+        k.segs.swap(segs);
+        k.seg_tasks.swap(tasks);
     }
     for (auto& k : t->keys)
         if (!jk_internal_batch_launcher(k.cls, 0))
@@ -219,6 +251,7 @@ static int batch_create(jk_basis_t* const* bases, int nmol, jk_batch* t) {
     BCUDA(cudaMalloc((void**)&t->d_cnt64, sizeof(long long*) * std::max(1, t->nseg)));
     BCUDA(cudaMalloc((void**)&t->d_cnt32, sizeof(long long*) * std::max(1, t->nseg)));
     BCUDA(cudaMalloc(&t->d_key_off, sizeof(int) * (nkeys + 1)));
+    BCUDA(cudaMalloc(&t->d_queue, sizeof(unsigned long long) * 2 * std::max(1, nkeys)));
     if (t->nseg) {
         BCUDA(cudaMemcpy((void*)t->d_cnt64, c64.data(), sizeof(long long*) * t->nseg, cudaMemcpyHostToDevice));
         BCUDA(cudaMemcpy((void*)t->d_cnt32, c32.data(), sizeof(long long*) * t->nseg, cudaMemcpyHostToDevice));
@@ -328,11 +361,10 @@ static int batch_segments(jk_batch* t, const double* const* dms, double* const* 
     return JK_OK;
 }
 
-extern "C" int jk_batch_build(jk_batch_t* t, const double* const* dms, double* const* vjs, double* const* vks,
-                              int n_dm, const jk_opts_t* opts, void* stream) {
-    if (!t || !dms || n_dm <= 0) return jk_internal_set_err(JK_ERR_ARG, "jk_batch_build: invalid arguments");
-    if (!vjs && !vks) return JK_OK;
-    cudaStream_t st = (cudaStream_t)stream;
+// everything before the class launches: segment tables, density
+// condensation, screening, task prefixes, pair-packed densities
+static int batch_prepare(jk_batch* t, const double* const* dms, double* const* vjs, double* const* vks, int n_dm,
+                         const jk_opts_t* opts, cudaStream_t st) {
     int rc = batch_segments(t, dms, vjs, vks, n_dm, st);
     if (rc) return rc;
     double tol = opts ? opts->direct_scf_tol : t->mols[0]->cutoff;
@@ -343,7 +375,7 @@ extern "C" int jk_batch_build(jk_batch_t* t, const double* const* dms, double* c
     jk_dm_cond_batch_kernel<<<g, 256, 0, st>>>(t->d_dmc);
     BCUDA(cudaGetLastError());
     if (t->ncq == 0) return JK_OK;
-    rc = jk_internal_screen(t->d_cq, t->ncq, tol, nbins, prescreen, fp32_cutoff, stream);
+    rc = jk_internal_screen(t->d_cq, t->ncq, tol, nbins, prescreen, fp32_cutoff, st);
     if (rc) return rc;
     int nkeys = (int)t->keys.size();
     jk_seg_prefix_kernel<<<nkeys, 32, 0, st>>>(t->d_cnt64, t->d_key_off, t->d_segt64);
@@ -353,26 +385,194 @@ extern "C" int jk_batch_build(jk_batch_t* t, const double* const* dms, double* c
         BCUDA(cudaGetLastError());
     }
     if (t->packed) {
-        rc = jk_internal_pack_batch(t->d_pmol, t->nmol, t->pk_max, 0, stream);
+        rc = jk_internal_pack_batch(t->d_pmol, t->nmol, t->pk_max, 0, st);
         if (rc) return rc;
         BCUDA(cudaMemsetAsync(t->d_pk + t->pk_jp, 0, sizeof(double) * t->pk_jp, st));
     }
+    return JK_OK;
+}
+
+// the class launch of key k, part 0 (FP64) or 1 (FP32), with shape cfg
+static int batch_launch_key(jk_batch* t, int k, int part, const JKBatchCfg& cfg, cudaStream_t st) {
+    const JKBatchKey& key = t->keys[k];
+    int off = t->key_off[k], n = t->key_off[k + 1] - off;
+    jk_launch_batch_fn f = jk_internal_batch_launcher(key.cls, part);
+    if (!f) return jk_internal_set_err(JK_ERR_UNSUPPORTED, "no kernel for a class of the batch");
+    JKBatchCfg c = cfg;
+    if (c.grab > 0) c.queue = t->d_queue + 2 * k + part;
+    else c.queue = nullptr;
+    const JKSeg* segs = (part ? t->d_seg32 : t->d_seg64) + off;
+    const long long* segt = (part ? t->d_segt32 : t->d_segt64) + off + k;
+    BCUDA(f(segs, segt, n, key.max_tasks, t->nsm, c, st));
+    return JK_OK;
+}
+
+extern "C" int jk_batch_build(jk_batch_t* t, const double* const* dms, double* const* vjs, double* const* vks,
+                              int n_dm, const jk_opts_t* opts, void* stream) {
+    if (!t || !dms || n_dm <= 0) return jk_internal_set_err(JK_ERR_ARG, "jk_batch_build: invalid arguments");
+    if (!vjs && !vks) return JK_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc = batch_prepare(t, dms, vjs, vks, n_dm, opts, st);
+    if (rc || t->ncq == 0) return rc;
+    const bool mixed = opts && opts->fp32_cutoff > 0;
+    int nkeys = (int)t->keys.size();
+    // work counters of the persistent launches start at zero every build
+    BCUDA(cudaMemsetAsync(t->d_queue, 0, sizeof(unsigned long long) * 2 * nkeys, st));
     BCUDA(t->fan.begin(st));
     for (int k = 0; k < nkeys; k++) {
-        const JKBatchKey& key = t->keys[k];
-        int off = t->key_off[k], n = t->key_off[k + 1] - off;
-        jk_launch_batch_fn f = jk_internal_batch_launcher(key.cls, 0);
-        BCUDA(f(t->d_seg64 + off, t->d_segt64 + off + k, n, key.max_tasks, t->nsm, t->fan.pick(2 * k)));
-        if (fp32_cutoff > 0) {
-            jk_launch_batch_fn f32 = jk_internal_batch_launcher(key.cls, 1);
-            if (!f32) return jk_internal_set_err(JK_ERR_UNSUPPORTED, "no FP32 kernel for a class");
-            BCUDA(f32(t->d_seg32 + off, t->d_segt32 + off + k, n, key.max_tasks, t->nsm, t->fan.pick(2 * k + 1)));
+        rc = batch_launch_key(t, k, 0, t->keys[k].cfg[0], t->fan.pick(2 * k));
+        if (rc) return rc;
+        if (mixed) {
+            rc = batch_launch_key(t, k, 1, t->keys[k].cfg[1], t->fan.pick(2 * k + 1));
+            if (rc) return rc;
         }
     }
     BCUDA(t->fan.end(st));
     if (t->packed) {
         rc = jk_internal_pack_batch(t->d_pmol, t->nmol, t->pk_max, 1, stream);
         if (rc) return rc;
+    }
+    return JK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner.  For every key (and both parts in the mixed mode) the candidate
+// launch shapes are timed on this batch with CUDA events, each launch alone
+// on the caller's stream after the bookkeeping of a real build, and the
+// fastest is kept.  Candidates: static chunks; the persistent mode at one
+// and two resident grids with three grab sizes (tasks per warp for the
+// thread kernels, per team for the team kernels, per block for the generic
+// kernel).  A cache file keeps the choices per (class, primitive counts,
+// part, log2 of the task count); keys found there are not timed again.
+// ---------------------------------------------------------------------------
+static bool class_is_generic(int cls) {
+    const int ll = cls % 7, lk = (cls / 7) % 7, lj = (cls / 49) % 7, li = cls / 343;
+    return li > JK_LMAX || lj > JK_LMAX || lk > JK_LMAX || ll > JK_LMAX;
+}
+
+static int cand_grabs(int cls, int* g) {
+    if (jk_internal_class_team(cls)) { g[0] = 2; g[1] = 8; g[2] = 32; }
+    else if (class_is_generic(cls)) { g[0] = 1; g[1] = 4; g[2] = 16; }
+    else { g[0] = 64; g[1] = 256; g[2] = 1024; }
+    return 3;
+}
+
+static std::string tune_key_str(const JKBatchKey& k, int part) {
+    int b = 0;
+    for (long long x = k.max_tasks; x > 1; x >>= 1) b++;
+    char buf[96];
+    snprintf(buf, sizeof(buf), "%d %d %d %d %d", k.cls, k.np_ij, k.np_kl, part, b);
+    return buf;
+}
+
+extern "C" int jk_batch_tune(jk_batch_t* t, const double* const* dms, double* const* vjs, double* const* vks,
+                             int n_dm, const jk_opts_t* opts, const char* cache_path, void* stream) {
+    if (!t || !dms || n_dm <= 0 || (!vjs && !vks))
+        return jk_internal_set_err(JK_ERR_ARG, "jk_batch_tune: invalid arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    int nkeys = (int)t->keys.size();
+    const bool mixed = opts && opts->fp32_cutoff > 0;
+    // cached choices: "cls np_ij np_kl part log2tasks mode grab grid_mul ms"
+    std::map<std::string, std::pair<JKBatchCfg, float>> cache;
+    if (cache_path) {
+        FILE* f = fopen(cache_path, "r");
+        if (f) {
+            char line[256];
+            while (fgets(line, sizeof(line), f)) {
+                int cls, a, b, part, lg, grab, gm;
+                float ms;
+                if (sscanf(line, "%d %d %d %d %d %d %d %f", &cls, &a, &b, &part, &lg, &grab, &gm, &ms) != 8) continue;
+                char key[96];
+                snprintf(key, sizeof(key), "%d %d %d %d %d", cls, a, b, part, lg);
+                cache[key] = {JKBatchCfg{nullptr, grab, gm}, ms};
+            }
+            fclose(f);
+        }
+    }
+    int rc = batch_prepare(t, dms, vjs, vks, n_dm, opts, st);
+    if (rc) return rc;
+    cudaEvent_t e0, e1;
+    BCUDA(cudaEventCreate(&e0));
+    BCUDA(cudaEventCreate(&e1));
+    for (int k = 0; k < nkeys && t->ncq; k++) {
+        JKBatchKey& key = t->keys[k];
+        for (int part = 0; part < (mixed ? 2 : 1); part++) {
+            const std::string ks = tune_key_str(key, part);
+            auto hit = cache.find(ks);
+            if (hit != cache.end()) {
+                key.cfg[part] = hit->second.first;
+                key.tuned_ms[part] = hit->second.second;
+                continue;
+            }
+            int g[3];
+            cand_grabs(key.cls, g);
+            std::vector<JKBatchCfg> cands = {{nullptr, 0, 1}};
+            for (int gm = 1; gm <= 2; gm++)
+                for (int i = 0; i < 3; i++) cands.push_back({nullptr, g[i], gm});
+            float best = -1.f;
+            for (const JKBatchCfg& c : cands) {
+                float tmin = -1.f;
+                for (int rep = 0; rep < 2; rep++) {
+                    BCUDA(cudaMemsetAsync(t->d_queue, 0, sizeof(unsigned long long) * 2 * nkeys, st));
+                    BCUDA(cudaEventRecord(e0, st));
+                    rc = batch_launch_key(t, k, part, c, st);
+                    if (rc) return rc;
+                    BCUDA(cudaEventRecord(e1, st));
+                    BCUDA(cudaEventSynchronize(e1));
+                    float ms = 0.f;
+                    BCUDA(cudaEventElapsedTime(&ms, e0, e1));
+                    if (tmin < 0 || ms < tmin) tmin = ms;
+                }
+                if (best < 0 || tmin < best) {
+                    best = tmin;
+                    key.cfg[part] = c;
+                }
+            }
+            key.tuned_ms[part] = best;
+            cache[ks] = {key.cfg[part], best};
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    BCUDA(cudaStreamSynchronize(st));
+    // the timing runs accumulated into the outputs: clear them
+    for (int m = 0; m < t->nmol; m++) {
+        size_t nn = (size_t)t->mols[m]->nao * t->mols[m]->nao * n_dm;
+        if (vjs && vjs[m]) BCUDA(cudaMemset(vjs[m], 0, sizeof(double) * nn));
+        if (vks && vks[m]) BCUDA(cudaMemset(vks[m], 0, sizeof(double) * nn));
+    }
+    if (cache_path) {
+        FILE* f = fopen(cache_path, "w");
+        if (!f) return jk_internal_set_err(JK_ERR_ARG, "jk_batch_tune: cannot write the cache file");
+        fprintf(f, "# byteqc_b200 batch launch shapes: cls np_ij np_kl part log2tasks grab grid_mul ms\n");
+        for (auto& kv : cache)
+            fprintf(f, "%s %d %d %.4f\n", kv.first.c_str(), kv.second.first.grab, kv.second.first.grid_mul,
+                    kv.second.second);
+        fclose(f);
+    }
+    return JK_OK;
+}
+
+// launch shapes chosen for the batch: per key cls, np_ij, np_kl, then for
+// parts 0 and 1 grab, grid_mul and the tuned time in microseconds (-1 if
+// not tuned); out holds 12 ints per key
+extern "C" int jk_batch_info(const jk_batch_t* t, int* nkeys, int* out) {
+    if (!t || !nkeys) return jk_internal_set_err(JK_ERR_ARG, "jk_batch_info: invalid arguments");
+    *nkeys = (int)t->keys.size();
+    if (!out) return JK_OK;
+    for (size_t k = 0; k < t->keys.size(); k++) {
+        const JKBatchKey& key = t->keys[k];
+        int* o = out + 12 * k;
+        o[0] = key.cls;
+        o[1] = key.np_ij;
+        o[2] = key.np_kl;
+        o[3] = (int)std::min<long long>(key.max_tasks, 2147483647LL);
+        for (int p = 0; p < 2; p++) {
+            o[4 + 4 * p] = key.cfg[p].grab;
+            o[5 + 4 * p] = key.cfg[p].grid_mul;
+            o[6 + 4 * p] = (int)(key.tuned_ms[p] * 1000.f);
+            o[7 + 4 * p] = (int)key.segs.size();
+        }
     }
     return JK_OK;
 }

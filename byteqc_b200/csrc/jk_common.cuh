@@ -12,10 +12,10 @@
 #include "rys_table.h"
 
 #define JK_LMAX 3      // angular momentum handled by the templated kernels
-#define JK_LMAX_ALL 5  // ... and by the generic kernel (jk_generic.cu): up to h
-// launcher tables are indexed by the class (li lj | lk ll), base 6
-#define JK_CLASS_INDEX(li, lj, lk, ll) ((((li) * 6 + (lj)) * 6 + (lk)) * 6 + (ll))
-#define JK_NCLASS 1296
+#define JK_LMAX_ALL 6  // ... and by the generic kernel (jk_generic.cu): up to i
+// launcher tables are indexed by the class (li lj | lk ll), base 7
+#define JK_CLASS_INDEX(li, lj, lk, ll) ((((li) * 7 + (lj)) * 7 + (lk)) * 7 + (ll))
+#define JK_NCLASS 2401
 
 // libcint slots (cuobc/lib/gint/gint.h:29-46)
 #define ATM_SLOTS 6
@@ -516,6 +516,14 @@ struct JKSeg {
     double* jp_ij;
     double* jp_kl;
     int np_ij, np_kl;        // pairs of each class (component stride)
+    // K through per-warp row buffers (jk_build's single-segment thread
+    // kernels, one density): first AO and AO count of the groups of the ket
+    // pair's two shells, and the buffer size per warp in doubles (0: off).
+    // rb_allowed: the caller accepts either orientation of a K element in
+    // the raw buffer (jk_build; the class-pair entries keep the reference's)
+    int kao0, nk, lao0, nl;
+    int rb_words;
+    int rb_allowed;
     long long pk_stride;     // packed elements per density
     int ls[4];               // angular momenta of the class (read by the generic kernel)
 };
@@ -523,6 +531,18 @@ struct JKSeg {
 // launchers of one class: a single segment (by value) or a segment table
 typedef cudaError_t (*jk_launch_fn)(const JKSeg& seg, const long long* task0, long long max_tasks, int nsm,
                                     cudaStream_t st);
+// Launch shape of one batched class launch (the knobs of the batch's
+// autotuner).  queue == nullptr: the tasks are split into equal contiguous
+// chunks over a grid sized by the unscreened task count.  Otherwise the
+// persistent mode: the grid is grid_mul x the kernel's resident blocks per
+// SM x the SMs, and the warps (thread kernels), teams (team kernels) or
+// blocks (generic kernel) take `grab` tasks at a time from the device
+// counter *queue, which the caller zeroes before the launch.
+struct JKBatchCfg {
+    unsigned long long* queue;
+    int grab;
+    int grid_mul;
+};
 typedef cudaError_t (*jk_launch_batch_fn)(const JKSeg* segs, const long long* segt, int nseg, long long max_tasks,
-                                          int nsm, cudaStream_t st);
+                                          int nsm, const JKBatchCfg& cfg, cudaStream_t st);
 

@@ -1,8 +1,13 @@
-// Generic J/K kernel for the classes with a shell above f (g and h, l = 4, 5),
-// with the angular momenta read at run time.  The reference's GPU kernels
-// reach h shells (cuobc/lib/gvhf/g2e.cu:32-996, up to 11 Rys roots), and
-// basis sets such as cc-pVQZ or def2-QZVP carry g functions.  These classes
-// are rare, so the kernel aims at correctness with bounded resources:
+// Generic J/K kernel for the classes with a shell above f (g, h and i,
+// l = 4, 5, 6), with the angular momenta read at run time.  The reference's
+// GPU kernels reach h shells (cuobc/lib/gvhf/g2e.cu:32-996, up to 11 Rys
+// roots) and hand quartets with an i shell to PySCF on the CPU
+// (cuobc/scf/hf.py:185-218); here i shells run on the GPU too (13 roots at
+// (ii|ii)).  Basis sets such as cc-pVQZ or def2-QZVP carry g functions,
+// cc-pV5Z h and cc-pV6Z i.  These classes are rare, so the kernel aims at
+// correctness with bounded resources; its fixed sizes come from the largest
+// l it serves, GL = 5 (every class up to (hh|hh), 86 KB of shared memory,
+// two CTAs per SM) or GL = 6 (classes with an i shell, 153 KB, one CTA):
 //
 //   one CTA per contracted quartet; for every primitive quartet and root the
 //   three (axis, root) 2D blocks are built in shared memory (threads 0-2),
@@ -18,10 +23,24 @@
 #include "jk_launch.cuh"
 
 #define JK_GEN_THREADS 128
-#define JK_GEN_NF 21    // Cartesian components of an h shell
-#define JK_GEN_GS 1296  // entries of one 2D block at (hh|hh): 6^4
-#define JK_GEN_NR 11    // roots at (hh|hh)
-#define JK_GEN_BLK (JK_GEN_NF * JK_GEN_NF)
+#define JK_FILL_CHUNK 4096
+
+// fixed sizes of the generic kernels serving shells up to l = GL
+template <int GL>
+struct JKGen {
+    static constexpr int NF = (GL + 1) * (GL + 2) / 2;              // Cartesian components of one shell
+    static constexpr int GS = (GL + 1) * (GL + 1) * (GL + 1) * (GL + 1);  // entries of one 2D block
+    static constexpr int NR = 2 * GL + 1;                           // roots of the largest class
+    static constexpr int BLK = NF * NF;
+    static constexpr int G1 = 2 * GL + 1;                           // VRR range in n and m
+    static constexpr int H1 = GL + 1;
+    static constexpr int W = G1 * G1 + H1 * H1 * G1 + 2 * G1;       // recursion scratch of one unit
+    static constexpr size_t SMEM = (3 * GS + 12 * BLK + 3 * W) * sizeof(double);
+    static constexpr size_t FILL_SMEM = (3 * GS + JK_FILL_CHUNK + 3 * W) * sizeof(double);
+    static constexpr size_t QC_SMEM = (3 * GS + BLK + 3 * W) * sizeof(double);
+    static constexpr int CTAS = GL <= 5 ? 2 : 1;                    // resident CTAs per SM
+};
+static_assert(JKGen<5>::SMEM <= 227 * 1024 && JKGen<6>::SMEM <= 227 * 1024, "generic kernel shared memory");
 
 // Rys node r at x with the root count N known at run time (the layout and
 // evaluation of rys_root<N>)
@@ -60,39 +79,40 @@ __device__ void rys_root_rt(const double* __restrict__ rys, int N, double x, int
 
 // One Rys 2D block at run-time angular momenta: the recursion of rys_2d,
 // output I[((i*(lj+1)+j)*(lk+1)+k)*(ll+1)+l].  The intermediate arrays live
-// in the caller's shared-memory scratch W (JK_GEN_W doubles), not on the
+// in the caller's shared-memory scratch W (JKGen<GL>::W doubles), not on the
 // thread's stack, which would reserve local memory for every resident thread
 // of the device.
-#define JK_GEN_W (11 * 11 + 6 * 6 * 11 + 2 * 11)
+template <int GL>
 __device__ void rys_2d_rt(int li, int lj, int lk, int ll, double seed, double c00, double c0p, double b10,
                           double b01, double b00, double dij, double dkl, double* __restrict__ W,
                           double* __restrict__ I) {
+    constexpr int G1 = JKGen<GL>::G1, H1 = JKGen<GL>::H1;
     const int nm = li + lj, mm = lk + ll;
-    double* G = W;                // G[n * 11 + m]
-    double* H = G + 11 * 11;      // H[(i * 6 + j) * 11 + m]: bra transfer
-    double* A = H + 6 * 6 * 11;
-    double* B = A + 11;
+    double* G = W;                // G[n * G1 + m]
+    double* H = G + G1 * G1;      // H[(i * H1 + j) * G1 + m]: bra transfer
+    double* A = H + H1 * H1 * G1;
+    double* B = A + G1;
     G[0] = seed;
-    for (int n = 0; n < nm; n++) G[(n + 1) * 11] = c00 * G[n * 11] + (n ? n * b10 * G[(n - 1) * 11] : 0.);
+    for (int n = 0; n < nm; n++) G[(n + 1) * G1] = c00 * G[n * G1] + (n ? n * b10 * G[(n - 1) * G1] : 0.);
     for (int m = 0; m < mm; m++)
         for (int n = 0; n <= nm; n++) {
-            double v = c0p * G[n * 11 + m];
-            if (m) v += m * b01 * G[n * 11 + m - 1];
-            if (n) v += n * b00 * G[(n - 1) * 11 + m];
-            G[n * 11 + m + 1] = v;
+            double v = c0p * G[n * G1 + m];
+            if (m) v += m * b01 * G[n * G1 + m - 1];
+            if (n) v += n * b00 * G[(n - 1) * G1 + m];
+            G[n * G1 + m + 1] = v;
         }
     const int SK = ll + 1, SJ = (lk + 1) * SK, SI = (lj + 1) * SJ;
     for (int m = 0; m <= mm; m++) {
-        for (int a = 0; a <= nm; a++) A[a] = G[a * 11 + m];
-        for (int i = 0; i <= li; i++) H[(i * 6) * 11 + m] = A[i];
+        for (int a = 0; a <= nm; a++) A[a] = G[a * G1 + m];
+        for (int i = 0; i <= li; i++) H[(i * H1) * G1 + m] = A[i];
         for (int j = 1; j <= lj; j++) {
             for (int a = 0; a + j <= nm; a++) A[a] = A[a + 1] + dij * A[a];
-            for (int i = 0; i <= li; i++) H[(i * 6 + j) * 11 + m] = A[i];
+            for (int i = 0; i <= li; i++) H[(i * H1 + j) * G1 + m] = A[i];
         }
     }
     for (int i = 0; i <= li; i++)  // ket transfer
         for (int j = 0; j <= lj; j++) {
-            for (int c = 0; c <= mm; c++) B[c] = H[(i * 6 + j) * 11 + c];
+            for (int c = 0; c <= mm; c++) B[c] = H[(i * H1 + j) * G1 + c];
             for (int k = 0; k <= lk; k++) I[i * SI + j * SJ + k * SK] = B[k];
             for (int l = 1; l <= ll; l++) {
                 for (int c = 0; c + l <= mm; c++) B[c] = B[c + 1] + dkl * B[c];
@@ -102,6 +122,7 @@ __device__ void rys_2d_rt(int li, int lj, int lk, int ll, double seed, double c0
 }
 
 // the (axis d, root) block of a primitive quartet (jk_unit at run-time l)
+template <int GL>
 __device__ void jk_unit_rt(const JKPrim& p, double s, double w, int d, double norm, const double* ri,
                            const double* rj, const double* rk, const double* rl, int li, int lj, int lk, int ll,
                            double* W, double* out) {
@@ -114,7 +135,7 @@ __device__ void jk_unit_rt(const JKPrim& p, double s, double w, int d, double no
     const double c00 = (p.P[d] - ri[d]) - bs * pq;
     const double c0p = (p.Q[d] - rk[d]) + as * pq;
     const double seed = d == 0 ? norm : (d == 1 ? p.sy : w);
-    rys_2d_rt(li, lj, lk, ll, seed, c00, c0p, b10, b01, b00, ri[d] - rj[d], rk[d] - rl[d], W, out);
+    rys_2d_rt<GL>(li, lj, lk, ll, seed, c00, c0p, b10, b01, b00, ri[d] - rj[d], rk[d] - rl[d], W, out);
 }
 
 // Cartesian exponents of the components of shell l into ex[c][3]
@@ -130,23 +151,34 @@ __device__ void jk_cart_table(int l, int (*ex)[3]) {
 // J/K of one class (one segment or a segment table), one quartet per CTA at
 // a time; each CTA takes a contiguous chunk of the tasks
 // ---------------------------------------------------------------------------
-template <class Src>
+template <int GL, class Src>
 __device__ void jk_generic_body(const Src& src) {
+    using G = JKGen<GL>;
     extern __shared__ __align__(16) double gsm[];
-    double* gI = gsm;                    // 3 x JK_GEN_GS: the blocks of one root
-    double* Dsm = gI + 3 * JK_GEN_GS;    // density blocks
-    double* acc = Dsm + 6 * JK_GEN_BLK;  // accumulator blocks
-    double* wk = acc + 6 * JK_GEN_BLK;   // 3 x JK_GEN_W: recursion scratch of threads 0-2
+    double* gI = gsm;                  // 3 x G::GS: the blocks of one root
+    double* Dsm = gI + 3 * G::GS;      // density blocks
+    double* acc = Dsm + 6 * G::BLK;    // accumulator blocks
+    double* wk = acc + 6 * G::BLK;     // 3 x G::W: recursion scratch of threads 0-2
     __shared__ JKQuartet s_q;
     __shared__ const JKSeg* s_sg;
     __shared__ double s_c[12];
     __shared__ JKPrim s_p;
-    __shared__ double s_rs[JK_GEN_NR], s_rw[JK_GEN_NR];
-    __shared__ int s_ex[4][JK_GEN_NF][3];  // Cartesian exponents of the four shells
+    __shared__ double s_rs[G::NR], s_rw[G::NR];
+    __shared__ int s_ex[4][G::NF][3];  // Cartesian exponents of the four shells
     const int tid = threadIdx.x;
     const long long total = src.total();
-    const long long chunk = (total + gridDim.x - 1) / gridDim.x;
-    const long long tbeg = (long long)blockIdx.x * chunk;
+    unsigned long long* queue = src.queue();
+    const long long chunk = queue ? (long long)src.grab() : (total + gridDim.x - 1) / gridDim.x;
+    __shared__ long long s_grab;
+    long long tbeg = (long long)blockIdx.x * chunk;
+    for (;;) {
+    if (queue) {  // persistent mode: the block takes `chunk` tasks per round
+        __syncthreads();
+        if (tid == 0) s_grab = (long long)atomicAdd(queue, (unsigned long long)chunk);
+        __syncthreads();
+        tbeg = s_grab;
+    }
+    if (tbeg >= total) break;
     const long long tend = min(total, tbeg + chunk);
     typename Src::Cursor cur;
     if (tid == 0 && tbeg < tend) cur.init(src, tbeg);
@@ -204,12 +236,12 @@ __device__ void jk_generic_body(const Src& src) {
                     __syncthreads();
                     for (int r = 0; r < nr; r++) {
                         if (tid < 3)
-                            jk_unit_rt(s_p, s_rs[r], s_rw[r], tid, q.norm, s_c, s_c + 3, s_c + 6, s_c + 9, li, lj,
-                                       lk, ll, wk + tid * JK_GEN_W, gI + tid * JK_GEN_GS);
+                            jk_unit_rt<GL>(s_p, s_rs[r], s_rw[r], tid, q.norm, s_c, s_c + 3, s_c + 6, s_c + 9, li,
+                                           lj, lk, ll, wk + tid * G::W, gI + tid * G::GS);
                         __syncthreads();
                         const double* gx = gI;
-                        const double* gy = gI + JK_GEN_GS;
-                        const double* gz = gI + 2 * JK_GEN_GS;
+                        const double* gy = gI + G::GS;
+                        const double* gz = gI + 2 * G::GS;
 #define JK_GEN_I(i, j, k, l)                                                                                  \
     (gx[s_ex[0][i][0] * SI + s_ex[1][j][0] * SJ + s_ex[2][k][0] * SK + s_ex[3][l][0]] *                       \
      gy[s_ex[0][i][1] * SI + s_ex[1][j][1] * SJ + s_ex[2][k][1] * SK + s_ex[3][l][1]] *                       \
@@ -264,54 +296,53 @@ __device__ void jk_generic_body(const Src& src) {
             __syncthreads();  // the shared buffers are reused by the next density / quartet
         }
     }
+    if (!queue) break;
+    }
 }
 
+template <int GL>
 __global__ void __launch_bounds__(JK_GEN_THREADS) jk_generic_kernel(const __grid_constant__ JKSeg sg,
                                                                     const long long* __restrict__ task0) {
     JKOneSeg src{sg, task0};
-    jk_generic_body(src);
+    jk_generic_body<GL>(src);
 }
 
+template <int GL>
 __global__ void __launch_bounds__(JK_GEN_THREADS) jk_generic_kernel_batch(const JKSeg* __restrict__ segs,
                                                                           const long long* __restrict__ segt,
-                                                                          int nseg) {
-    JKSegTable src{segs, segt, nseg};
-    jk_generic_body(src);
+                                                                          int nseg, unsigned long long* queue,
+                                                                          int grab) {
+    JKSegTable src{segs, segt, nseg, queue, grab};
+    jk_generic_body<GL>(src);
 }
 
-static constexpr size_t JK_GEN_SMEM = (3 * JK_GEN_GS + 12 * JK_GEN_BLK + 3 * JK_GEN_W) * sizeof(double);
-
-static cudaError_t jk_generic_attr() {
-    // per device: the attribute is set on the current device's function
-    cudaError_t e = cudaFuncSetAttribute(jk_generic_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)JK_GEN_SMEM);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(jk_generic_kernel_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)JK_GEN_SMEM);
-    return e;
-}
-
+template <int GL>
 static int jk_generic_blocks(long long max_tasks, int nsm) {
-    const long long cap = (long long)nsm * 2;  // two 86 KB CTAs per SM
+    const long long cap = (long long)nsm * JKGen<GL>::CTAS;
     return (int)(max_tasks < cap ? max_tasks : cap);
 }
 
+template <int GL>
 static cudaError_t jk_launch_generic(const JKSeg& seg, const long long* task0, long long max_tasks, int nsm,
                                      cudaStream_t st) {
     if (max_tasks <= 0) return cudaSuccess;
-    cudaError_t e = jk_generic_attr();
-    if (e != cudaSuccess) return e;
-    jk_generic_kernel<<<jk_generic_blocks(max_tasks, nsm), JK_GEN_THREADS, JK_GEN_SMEM, st>>>(seg, task0);
+    static std::atomic<unsigned long long> attr_done{0};
+    if (cudaError_t e = jk_smem_attr(jk_generic_kernel<GL>, JKGen<GL>::SMEM, attr_done); e != cudaSuccess) return e;
+    jk_generic_kernel<GL><<<jk_generic_blocks<GL>(max_tasks, nsm), JK_GEN_THREADS, JKGen<GL>::SMEM, st>>>(seg,
+                                                                                                         task0);
     return cudaGetLastError();
 }
 
+template <int GL>
 static cudaError_t jk_launch_generic_batch(const JKSeg* segs, const long long* segt, int nseg, long long max_tasks,
-                                           int nsm, cudaStream_t st) {
+                                           int nsm, const JKBatchCfg& cfg, cudaStream_t st) {
     if (max_tasks <= 0 || nseg <= 0) return cudaSuccess;
-    cudaError_t e = jk_generic_attr();
-    if (e != cudaSuccess) return e;
-    jk_generic_kernel_batch<<<jk_generic_blocks(max_tasks, nsm), JK_GEN_THREADS, JK_GEN_SMEM, st>>>(segs, segt,
-                                                                                                    nseg);
+    static std::atomic<unsigned long long> attr_done{0};
+    if (cudaError_t e = jk_smem_attr(jk_generic_kernel_batch<GL>, JKGen<GL>::SMEM, attr_done); e != cudaSuccess)
+        return e;
+    const int blocks = cfg.queue ? nsm * JKGen<GL>::CTAS * cfg.grid_mul : jk_generic_blocks<GL>(max_tasks, nsm);
+    jk_generic_kernel_batch<GL><<<blocks, JK_GEN_THREADS, JKGen<GL>::SMEM, st>>>(segs, segt, nseg, cfg.queue,
+                                                                                cfg.grab);
     return cudaGetLastError();
 }
 
@@ -323,31 +354,26 @@ static cudaError_t jk_launch_generic_batch(const JKSeg* segs, const long long* s
 // the working basis).  Every class up to (hh|hh); one CTA per quartet; the
 // quartet's integrals are summed over primitives and roots in a shared-memory
 // chunk of up to JK_FILL_CHUNK elements (classes with more components run
-// the primitive loop once per chunk), then added to the tensor.  The
+// the primitive loop once per chunk), then added to the tensor (classes
+// with an i shell use the GL = 6 sizes).  The
 // integrals carry no 1/2 on the ij == kl diagonal (that factor belongs to
 // the J/K digestion); pairs on the diagonal of a shell carry the basis
 // handle's diagonal factor, as the reference's pair data do.
 // ---------------------------------------------------------------------------
-#define JK_FILL_CHUNK 4096
-
-struct JKFillOut {
-    double* eri;
-    long long st[4];
-    int off[4];
-};
-
+template <int GL>
 __global__ void __launch_bounds__(JK_GEN_THREADS) jk_fill_kernel(const __grid_constant__ JKSeg sg,
                                                                  const long long* __restrict__ task0,
                                                                  const JKFillOut out) {
+    using G = JKGen<GL>;
     extern __shared__ __align__(16) double gsm[];
-    double* gI = gsm;                     // 3 x JK_GEN_GS: the blocks of one root
-    double* acc = gI + 3 * JK_GEN_GS;     // JK_FILL_CHUNK integrals of the quartet
-    double* wk = acc + JK_FILL_CHUNK;     // 3 x JK_GEN_W: recursion scratch of threads 0-2
+    double* gI = gsm;                     // 3 x G::GS: the blocks of one root
+    double* acc = gI + 3 * G::GS;         // JK_FILL_CHUNK integrals of the quartet
+    double* wk = acc + JK_FILL_CHUNK;     // 3 x G::W: recursion scratch of threads 0-2
     __shared__ JKQuartet s_q;
     __shared__ double s_c[12];
     __shared__ JKPrim s_p;
-    __shared__ double s_rs[JK_GEN_NR], s_rw[JK_GEN_NR];
-    __shared__ int s_ex[4][JK_GEN_NF][3];
+    __shared__ double s_rs[G::NR], s_rw[G::NR];
+    __shared__ int s_ex[4][G::NF][3];
     const int tid = threadIdx.x;
     const long long total = task0[1];
     const long long chunk = (total + gridDim.x - 1) / gridDim.x;
@@ -385,8 +411,8 @@ __global__ void __launch_bounds__(JK_GEN_THREADS) jk_fill_kernel(const __grid_co
                     __syncthreads();
                     for (int r = 0; r < nr; r++) {
                         if (tid < 3)
-                            jk_unit_rt(s_p, s_rs[r], s_rw[r], tid, JK_FAC, s_c, s_c + 3, s_c + 6, s_c + 9, li, lj, lk,
-                                       ll, wk + tid * JK_GEN_W, gI + tid * JK_GEN_GS);
+                            jk_unit_rt<GL>(s_p, s_rs[r], s_rw[r], tid, JK_FAC, s_c, s_c + 3, s_c + 6, s_c + 9, li,
+                                           lj, lk, ll, wk + tid * G::W, gI + tid * G::GS);
                         __syncthreads();
                         for (int e = c0 + tid; e < c1; e += JK_GEN_THREADS) {
                             int x = e;
@@ -398,7 +424,7 @@ __global__ void __launch_bounds__(JK_GEN_THREADS) jk_fill_kernel(const __grid_co
                             const int i = x / nfj;
                             double v = 1.;
                             for (int d = 0; d < 3; d++)
-                                v *= gI[d * JK_GEN_GS + s_ex[0][i][d] * SI + s_ex[1][j][d] * SJ + s_ex[2][k][d] * SK +
+                                v *= gI[d * G::GS + s_ex[0][i][d] * SI + s_ex[1][j][d] * SJ + s_ex[2][k][d] * SK +
                                         s_ex[3][l][d]];
                             acc[e - c0] += v;
                         }
@@ -424,24 +450,39 @@ __global__ void __launch_bounds__(JK_GEN_THREADS) jk_fill_kernel(const __grid_co
     }
 }
 
-static constexpr size_t JK_FILL_SMEM = (3 * JK_GEN_GS + JK_FILL_CHUNK + 3 * JK_GEN_W) * sizeof(double);
+template <int GL>
+static cudaError_t jk_launch_fill_gl(const JKSeg& seg, const long long* task0, long long max_tasks, int nsm,
+                                     const JKFillOut& out, cudaStream_t st) {
+    static std::atomic<unsigned long long> attr_done{0};
+    if (cudaError_t e = jk_smem_attr(jk_fill_kernel<GL>, JKGen<GL>::FILL_SMEM, attr_done); e != cudaSuccess)
+        return e;
+    const long long cap = (long long)nsm * 2;  // two CTAs per SM (77 KB at GL = 5, 110 KB at GL = 6)
+    const int blocks = (int)(max_tasks < cap ? max_tasks : cap);
+    jk_fill_kernel<GL><<<blocks, JK_GEN_THREADS, JKGen<GL>::FILL_SMEM, st>>>(seg, task0, out);
+    return cudaGetLastError();
+}
 
+jk_fill_fn jk_internal_fill_launcher(int class_idx);
+
+// classes up to f with a templated kernel use it (the thread or team shape
+// of their J/K kernel, writing the quartet's block instead of digesting
+// it); the others the generic kernel above
 cudaError_t jk_launch_fill(const JKSeg& seg, const long long* task0, long long max_tasks, int nsm, double* eri,
                            const long long* strides, const int* offsets, cudaStream_t st) {
     if (max_tasks <= 0) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(jk_fill_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)JK_FILL_SMEM);
-    if (e != cudaSuccess) return e;
     JKFillOut out;
     out.eri = eri;
     for (int a = 0; a < 4; a++) {
         out.st[a] = strides[a];
         out.off[a] = offsets[a];
     }
-    const long long cap = (long long)nsm * 2;  // two 77 KB CTAs per SM
-    const int blocks = (int)(max_tasks < cap ? max_tasks : cap);
-    jk_fill_kernel<<<blocks, JK_GEN_THREADS, JK_FILL_SMEM, st>>>(seg, task0, out);
-    return cudaGetLastError();
+    const int lmax = max(max(seg.ls[0], seg.ls[1]), max(seg.ls[2], seg.ls[3]));
+    if (lmax <= JK_LMAX) {
+        jk_fill_fn f = jk_internal_fill_launcher(JK_CLASS_INDEX(seg.ls[0], seg.ls[1], seg.ls[2], seg.ls[3]));
+        if (f) return f(seg, task0, max_tasks, nsm, out, st);
+    }
+    return lmax <= 5 ? jk_launch_fill_gl<5>(seg, task0, max_tasks, nsm, out, st)
+                     : jk_launch_fill_gl<6>(seg, task0, max_tasks, nsm, out, st);
 }
 
 // every class with a shell above f runs the generic kernel, in FP64 also for
@@ -453,8 +494,9 @@ void jk_register_generic(JKTables* T) {
                 for (int ll = 0; ll <= lk; ll++) {
                     if (li <= JK_LMAX && lk <= JK_LMAX) continue;
                     const int c = JK_CLASS_INDEX(li, lj, lk, ll);
-                    T->t64[c] = T->t32[c] = jk_launch_generic;
-                    T->b64[c] = T->b32[c] = jk_launch_generic_batch;
+                    const bool six = li == 6 || lk == 6;  // li >= lj, lk >= ll
+                    T->t64[c] = T->t32[c] = six ? jk_launch_generic<6> : jk_launch_generic<5>;
+                    T->b64[c] = T->b32[c] = six ? jk_launch_generic_batch<6> : jk_launch_generic_batch<5>;
                 }
 }
 
@@ -463,17 +505,19 @@ void jk_register_generic(JKTables* T) {
 // (the quantity jk_qcond_kernel gives the lower classes): one CTA per pair,
 // the diagonal elements owned by the threads
 // ---------------------------------------------------------------------------
+template <int GL>
 __global__ void __launch_bounds__(JK_GEN_THREADS) jk_qcond_generic_kernel(
     const int* __restrict__ pi, const int* __restrict__ pj, int npairs, const int* __restrict__ atm,
     const int* __restrict__ bas, const double* __restrict__ env, int nbas, double* __restrict__ q,
     const double* __restrict__ rys) {
+    using G = JKGen<GL>;
     extern __shared__ __align__(16) double gsm[];
     double* gI = gsm;
-    double* diag = gI + 3 * JK_GEN_GS;
-    double* wk = diag + JK_GEN_BLK;
+    double* diag = gI + 3 * G::GS;
+    double* wk = diag + G::BLK;
     __shared__ JKPrim s_p;
-    __shared__ double s_rs[JK_GEN_NR], s_rw[JK_GEN_NR], s_c[6];
-    __shared__ int s_ex[2][JK_GEN_NF][3];
+    __shared__ double s_rs[G::NR], s_rw[G::NR], s_c[6];
+    __shared__ int s_ex[2][G::NF][3];
     __shared__ double s_red[JK_GEN_THREADS];
     const int tid = threadIdx.x;
     for (int p = blockIdx.x; p < npairs; p += gridDim.x) {
@@ -530,14 +574,14 @@ __global__ void __launch_bounds__(JK_GEN_THREADS) jk_qcond_generic_kernel(
                         __syncthreads();
                         for (int r = 0; r < nr; r++) {
                             if (tid < 3)
-                                jk_unit_rt(s_p, s_rs[r], s_rw[r], tid, JK_FAC, s_c, s_c + 3, s_c, s_c + 3, li, lj,
-                                           li, lj, wk + tid * JK_GEN_W, gI + tid * JK_GEN_GS);
+                                jk_unit_rt<GL>(s_p, s_rs[r], s_rw[r], tid, JK_FAC, s_c, s_c + 3, s_c, s_c + 3, li,
+                                               lj, li, lj, wk + tid * G::W, gI + tid * G::GS);
                             __syncthreads();
                             for (int e = tid; e < nfi * nfj; e += JK_GEN_THREADS) {
                                 const int a = e / nfj, b = e - a * nfj;
                                 double v = 1.;
                                 for (int d = 0; d < 3; d++)
-                                    v *= gI[d * JK_GEN_GS + s_ex[0][a][d] * (SI + SK) + s_ex[1][b][d] * (SJ + 1)];
+                                    v *= gI[d * G::GS + s_ex[0][a][d] * (SI + SK) + s_ex[1][b][d] * (SJ + 1)];
                                 diag[e] += v;
                             }
                             __syncthreads();
@@ -560,14 +604,23 @@ __global__ void __launch_bounds__(JK_GEN_THREADS) jk_qcond_generic_kernel(
     }
 }
 
-void jk_qcond_generic(const int* pi, const int* pj, int n, const int* atm, const int* bas, const double* env,
-                      int nbas, double* q, const double* rys, cudaStream_t st) {
-    if (n <= 0) return;
-    const size_t smem = (3 * JK_GEN_GS + JK_GEN_BLK + 3 * JK_GEN_W) * sizeof(double);
+template <int GL>
+static void jk_qcond_generic_gl(const int* pi, const int* pj, int n, const int* atm, const int* bas,
+                                const double* env, int nbas, double* q, const double* rys, cudaStream_t st) {
+    static std::atomic<unsigned long long> attr_done{0};
     // a failure here shows up in the caller's cudaGetLastError
-    if (cudaFuncSetAttribute(jk_qcond_generic_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess)
-        return;
+    if (jk_smem_attr(jk_qcond_generic_kernel<GL>, JKGen<GL>::QC_SMEM, attr_done) != cudaSuccess) return;
     const int blocks = n < 4096 ? n : 4096;
-    jk_qcond_generic_kernel<<<blocks, JK_GEN_THREADS, smem, st>>>(pi, pj, n, atm, bas, env, nbas, q, rys);
+    jk_qcond_generic_kernel<GL><<<blocks, JK_GEN_THREADS, JKGen<GL>::QC_SMEM, st>>>(pi, pj, n, atm, bas, env, nbas,
+                                                                                   q, rys);
+}
+
+// lmax: the larger angular momentum of the pairs in the list (4..6)
+void jk_qcond_generic(const int* pi, const int* pj, int n, const int* atm, const int* bas, const double* env,
+                      int nbas, double* q, const double* rys, int lmax, cudaStream_t st) {
+    if (n <= 0) return;
+    if (lmax <= 5)
+        jk_qcond_generic_gl<5>(pi, pj, n, atm, bas, env, nbas, q, rys, st);
+    else
+        jk_qcond_generic_gl<6>(pi, pj, n, atm, bas, env, nbas, q, rys, st);
 }

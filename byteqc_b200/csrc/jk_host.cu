@@ -144,9 +144,10 @@ __global__ void jk_qcond_kernel(const int* __restrict__ pi, const int* __restric
     q[(size_t)jsh * nbas + ish] = v;
 }
 
-// Schwarz diagonal of pairs with a shell above f (jk_generic.cu)
+// Schwarz diagonal of pairs with a shell above f (jk_generic.cu); lmax is
+// the larger l of the pairs in the list
 void jk_qcond_generic(const int* pi, const int* pj, int n, const int* atm, const int* bas, const double* env,
-                      int nbas, double* q, const double* rys, cudaStream_t st);
+                      int nbas, double* q, const double* rys, int lmax, cudaStream_t st);
 
 typedef void (*qcond_fn)(const int*, const int*, int, const int*, const int*, const double*, int, double*,
                          const double*, cudaStream_t);
@@ -539,7 +540,7 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
                 if (a <= JK_LMAX)
                     g_qcond[a][c](dpi, dpj, n, b->d_atm, b->d_bas, b->d_env, nbas, b->d_qcond, b->rys, 0);
                 else
-                    jk_qcond_generic(dpi, dpj, n, b->d_atm, b->d_bas, b->d_env, nbas, b->d_qcond, b->rys, 0);
+                    jk_qcond_generic(dpi, dpj, n, b->d_atm, b->d_bas, b->d_env, nbas, b->d_qcond, b->rys, a, 0);
                 cudaError_t e = cudaGetLastError();
                 if (e == cudaSuccess) e = cudaDeviceSynchronize();
                 cudaFree(dpi);
@@ -693,6 +694,15 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
             c.qoff_off = b->qoff_total;
             b->qoff_total += c.n_ij + 1;
             b->h_cq.push_back(c);
+            // unscreened work for shard plans: quartets x primitive
+            // quartets x roots x Cartesian components (+ the digestion)
+            const int l4[4] = {b->h_group_l[c.gi], b->h_group_l[c.gj], b->h_group_l[c.gk], b->h_group_l[c.gl]};
+            double nf = 1.;
+            for (int a = 0; a < 4; a++) nf *= (l4[a] + 1) * (l4[a] + 2) / 2;
+            const double nq = cij == ckl ? 0.5 * c.n_ij * (c.n_ij + 1.) : (double)c.n_ij * c.n_kl;
+            const double npq = (double)b->h_group_nprim[c.gi] * b->h_group_nprim[c.gj] * b->h_group_nprim[c.gk] *
+                               b->h_group_nprim[c.gl];
+            b->h_cq_cost.push_back(nq * (npq * ((l4[0] + l4[1] + l4[2] + l4[3]) / 2 + 1) * nf + 12. * nf));
         }
     b->ncq = (int)b->h_cq.size();
     CUDA_TRY(cudaMalloc(&b->d_qoff, sizeof(long long) * (b->qoff_total ? b->qoff_total : 1)));
@@ -823,6 +833,15 @@ static void fill_seg(const jk_basis* b, int cp_ij, int cp_kl, const long long* q
     s->jp_ij = s->jp_kl = nullptr;
     s->np_ij = s->np_kl = 0;
     s->pk_stride = 0;
+    {
+        const int gk = b->h_cls_gi[cp_kl], gl = b->h_cls_gj[cp_kl];
+        s->kao0 = b->h_ao_loc[b->h_group_off[gk]];
+        s->nk = b->h_ao_loc[b->h_group_off[gk + 1]] - s->kao0;
+        s->lao0 = b->h_ao_loc[b->h_group_off[gl]];
+        s->nl = b->h_ao_loc[b->h_group_off[gl + 1]] - s->lao0;
+        s->rb_words = 0;
+        s->rb_allowed = 0;
+    }
     s->ls[0] = b->h_group_l[b->h_cls_gi[cp_ij]];
     s->ls[1] = b->h_group_l[b->h_cls_gj[cp_ij]];
     s->ls[2] = b->h_group_l[b->h_cls_gi[cp_kl]];
@@ -834,6 +853,33 @@ static int class_index(const jk_basis* b, int cp_ij, int cp_kl) {
     int li = b->h_group_l[b->h_cls_gi[cp_ij]], lj = b->h_group_l[b->h_cls_gj[cp_ij]];
     int lk = b->h_group_l[b->h_cls_gi[cp_kl]], ll = b->h_group_l[b->h_cls_gj[cp_kl]];
     return JK_CLASS_INDEX(li, lj, lk, ll);
+}
+
+extern "C" int jk_shard_plan(const double* cost, int n, int nshards, int* owner) {
+    if (n < 0 || nshards < 1 || (n > 0 && (!cost || !owner)))
+        return set_err(JK_ERR_ARG, "jk_shard_plan: invalid arguments");
+    std::vector<int> ord(n);
+    for (int i = 0; i < n; i++) ord[i] = i;
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int c) { return cost[a] > cost[c]; });
+    std::vector<double> load(nshards, 0.);
+    for (int i : ord) {
+        int best = 0;
+        for (int r = 1; r < nshards; r++)
+            if (load[r] < load[best]) best = r;
+        owner[i] = best;
+        load[best] += cost[i];
+    }
+    return JK_OK;
+}
+
+// owner of every class quartet for nshards shards (cached per basis)
+static const int* shard_owners(jk_basis* b, int nshards) {
+    if (b->cq_owner_n != nshards || (int)b->h_cq_owner.size() != b->ncq) {
+        b->h_cq_owner.assign(b->ncq, 0);
+        jk_shard_plan(b->h_cq_cost.data(), b->ncq, nshards, b->h_cq_owner.data());
+        b->cq_owner_n = nshards;
+    }
+    return b->h_cq_owner.data();
 }
 
 extern "C" int jk_build(jk_basis_t* b, const double* dm, int n_dm, double* vj, double* vk, const jk_opts_t* opts,
@@ -870,11 +916,17 @@ extern "C" int jk_build(jk_basis_t* b, const double* dm, int n_dm, double* vj, d
         CUDA_TRY(cudaGetLastError());
         CUDA_TRY(cudaMemsetAsync(jp, 0, sizeof(double) * n_dm * b->pack_total, st));
     }
+    const int nshards = opts && opts->nshards > 1 ? opts->nshards : 1;
+    const int shard = opts ? opts->shard : 0;
+    if (nshards > 1 && (shard < 0 || shard >= nshards)) return set_err(JK_ERR_ARG, "jk_build: shard out of range");
+    const int* owner = nshards > 1 ? shard_owners(b, nshards) : nullptr;
     CUDA_TRY(b->fan.begin(st));
     for (int c = 0; c < b->ncq; c++) {
+        if (owner && owner[c] != shard) continue;
         const JKScreenCQ& cq = b->h_cq[c];
         JKSeg seg;
         fill_seg(b, cq.cp_ij, cq.cp_kl, b->d_qoff + cq.qoff_off, cq.n_ij, dm, n_dm, vj, vk, &seg);
+        seg.rb_allowed = 1;
         if (packed) {
             const JKPackCls &ki = b->h_pack[cq.cp_ij], &kk = b->h_pack[cq.cp_kl];
             seg.dp_ij = dp + ki.off;
@@ -1274,6 +1326,16 @@ int jk_internal_class_index(const jk_basis_t* b, int cp_ij, int cp_kl) { return 
 jk_launch_batch_fn jk_internal_batch_launcher(int class_idx, int fp32) {
     init_tables();
     return fp32 ? g_tabs.b32[class_idx] : g_tabs.b64[class_idx];
+}
+
+int jk_internal_class_team(int class_idx) {
+    init_tables();
+    return g_tabs.team[class_idx];
+}
+
+jk_fill_fn jk_internal_fill_launcher(int class_idx) {
+    init_tables();
+    return g_tabs.fill[class_idx];
 }
 
 void jk_internal_fill_seg_batch(const jk_basis_t* b, int c, const double* dm, int n_dm, double* vj, double* vk,

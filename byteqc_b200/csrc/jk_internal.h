@@ -113,6 +113,9 @@ struct jk_basis {
     std::vector<int> h_cls_gi, h_cls_gj, h_pair_locs, h_prim_locs, h_pair2bra, h_pair2ket;
     std::vector<double> h_log_q, h_log_q_raw, h_qcond;
     std::vector<JKScreenCQ> h_cq;
+    std::vector<double> h_cq_cost;     // unscreened work of each class quartet (shard plans)
+    std::vector<int> h_cq_owner;       // owner of each class quartet in the plan of
+    int cq_owner_n = 0;                // cq_owner_n shards
     std::vector<long long> h_qoff_off;
     long long qoff_total = 0;
     // device
@@ -153,6 +156,8 @@ struct jk_basis {
 // launch one class quartet of basis b as a single segment
 int jk_internal_class_index(const jk_basis_t* b, int cp_ij, int cp_kl);
 jk_launch_batch_fn jk_internal_batch_launcher(int class_idx, int fp32);
+// 1 if the class runs a team kernel (one primitive count per launch)
+int jk_internal_class_team(int class_idx);
 void jk_internal_fill_seg_batch(const jk_basis_t* b, int c, const double* dm, int n_dm, double* vj, double* vk,
                                 int fp32, JKSeg* out);
 // pack (mode 0) or unpack (mode 1) the J side of nmol molecules (device table)

@@ -69,6 +69,16 @@ __device__ __forceinline__ JKQuartet jk_quartet_at(const JKSeg& sg, int row, int
     return q;
 }
 
+// Output of the ERI-tensor fill (the reference's GINTfill_int2e,
+// cuobc/lib/gint/nr_fill_ao_ints.cu:493-549): element (a, b, c, d) of the
+// working basis at eri[(a - off[0]) st[0] + (b - off[1]) st[1] + (c - off[2])
+// st[2] + (d - off[3]) st[3]].
+struct JKFillOut {
+    double* eri;
+    long long st[4];
+    int off[4];
+};
+
 // Walks the tasks t = t0, t0 + step, ... of one segment in increasing order,
 // keeping the (row, row start, row end) of the last task so that each step
 // costs a few comparisons instead of a binary search over the rows.
@@ -97,9 +107,12 @@ struct JKTaskCursor {
 // prefix segt[0..nseg]; all segments of a launch share the class and the
 // primitive counts.  Cursors walk increasing task indices.
 struct JKOneSeg {
+    static constexpr bool ROWBUF = true;  // may digest K through row buffers
     const JKSeg& sg;
     const long long* task0;
     __device__ __forceinline__ long long total() const { return task0[1]; }
+    __device__ __forceinline__ unsigned long long* queue() const { return nullptr; }
+    __device__ __forceinline__ int grab() const { return 0; }
     __device__ __forceinline__ const JKSeg& first() const { return sg; }
     struct Cursor {
         JKTaskCursor rc;
@@ -110,14 +123,27 @@ struct JKOneSeg {
             row = rc.row;
             return src.sg;
         }
+        // one past the last task of the current row
+        __device__ __forceinline__ long long row_end() const { return rc.rend; }
     };
 };
 
+// Persistent mode (queue != nullptr): the grid is the resident capacity of
+// the device and its warps (thread kernels) or blocks (team and generic
+// kernels) take chunks of `grab` consecutive tasks from the device counter
+// *queue (zeroed before the launch) until the tasks run out; there is no
+// waiting on other blocks, only an atomic add per chunk.  Otherwise the
+// tasks are split into equal contiguous chunks over the grid.
 struct JKSegTable {
+    static constexpr bool ROWBUF = false;
     const JKSeg* segs;
     const long long* segt;
     int nseg;
+    unsigned long long* q;
+    int g;
     __device__ __forceinline__ long long total() const { return segt[nseg]; }
+    __device__ __forceinline__ unsigned long long* queue() const { return q; }
+    __device__ __forceinline__ int grab() const { return g; }
     __device__ __forceinline__ const JKSeg& first() const { return segs[0]; }
     struct Cursor {
         int s;
@@ -140,6 +166,7 @@ struct JKSegTable {
             row = rc.row;
             return src.segs[s];
         }
+        __device__ __forceinline__ long long row_end() const { return sbeg + rc.rend; }
     };
 };
 
@@ -334,9 +361,32 @@ __device__ __forceinline__ JKSinkGlobal jk_sink_global(const JKSeg& sg) {
     return JKSinkGlobal{sg.vj, sg.vk, sg.nao, (size_t)sg.nao * sg.nao};
 }
 
+// ---------------------------------------------------------------------------
+// K through per-warp row buffers.  While the lanes of a warp work on
+// quartets of one bra pair (ij) -- a warp takes consecutive columns of a
+// row -- every K contribution of those quartets lands in the rows i and j
+// of K, at the columns of the ket shells' two groups; the density elements
+// they need sit in the same rows of D.  The warp stages D(i, .) and D(j, .)
+// over those columns in shared memory when it enters the row, adds the K
+// contributions into shared-memory rows K(i, .) and K(j, .) (shared-memory
+// atomics: lanes may share a ket shell), and flushes them to global memory
+// with coalesced atomics when it leaves the row, instead of one scattered
+// global atomic and one scattered density load per element and quartet.
+// Layout per warp (doubles, W = nk + nl columns: the k group, then the l
+// group): D rows of i (NFI), D rows of j (NFJ), K rows of i, K rows of j.
+// ---------------------------------------------------------------------------
+struct JKRowBuf {
+    double* base;  // the warp's buffer, or null
+    int W;         // columns per row
+    int kc, lc;    // first column of this quartet's k and l shells
+    bool on;       // this lane digests K through the buffer
+};
+
+#define JK_RB_MIN_TASKS 128  // a row is buffered if this many of its tasks remain in the warp's chunk
+
 template <class C, typename R, int NI, class Sink>
 __device__ __forceinline__ void jk_thread_digest(const JKSeg& sg, const JKQuartet& q, int CI0, const R* acc,
-                                                 const Sink& sink) {
+                                                 const Sink& sink, const JKRowBuf& rb) {
     const int nao = sg.nao;
     const int i0 = q.i0 + CI0, j0 = q.j0;
     const int k0 = q.k0, l0 = q.l0;
@@ -422,7 +472,57 @@ __device__ __forceinline__ void jk_thread_digest(const JKSeg& sg, const JKQuarte
                     sink.jkl(idm, k0 + k, l0 + l, v);
                 }
         }
-        if (sg.vk) {
+        if (sg.vk && rb.on && idm == 0) {
+            const int W = rb.W;
+            const double* Di = rb.base;
+            const double* Dj = Di + C::NFI * W;
+            double* Ki = rb.base + (C::NFI + C::NFJ) * W;
+            double* Kj = Ki + C::NFI * W;
+#pragma unroll
+            for (int i = 0; i < NI; i++)
+#pragma unroll
+                for (int k = 0; k < C::NFK; k++) {  // K_ik += (ij|kl) D_jl
+                    double v = 0;
+#pragma unroll
+                    for (int j = 0; j < C::NFJ; j++)
+#pragma unroll
+                        for (int l = 0; l < C::NFL; l++) v += ACC(i, j, k, l) * Dj[j * W + rb.lc + l];
+                    atomicAdd(Ki + (CI0 + i) * W + rb.kc + k, v);
+                }
+#pragma unroll
+            for (int i = 0; i < NI; i++)
+#pragma unroll
+                for (int l = 0; l < C::NFL; l++) {  // K_il += (ij|kl) D_jk
+                    double v = 0;
+#pragma unroll
+                    for (int j = 0; j < C::NFJ; j++)
+#pragma unroll
+                        for (int k = 0; k < C::NFK; k++) v += ACC(i, j, k, l) * Dj[j * W + rb.kc + k];
+                    atomicAdd(Ki + (CI0 + i) * W + rb.lc + l, v);
+                }
+#pragma unroll
+            for (int j = 0; j < C::NFJ; j++)
+#pragma unroll
+                for (int k = 0; k < C::NFK; k++) {  // K_jk += (ij|kl) D_il
+                    double v = 0;
+#pragma unroll
+                    for (int i = 0; i < NI; i++)
+#pragma unroll
+                        for (int l = 0; l < C::NFL; l++) v += ACC(i, j, k, l) * Di[(CI0 + i) * W + rb.lc + l];
+                    atomicAdd(Kj + j * W + rb.kc + k, v);
+                }
+#pragma unroll
+            for (int j = 0; j < C::NFJ; j++)
+#pragma unroll
+                for (int l = 0; l < C::NFL; l++) {  // K_jl += (ij|kl) D_ik
+                    double v = 0;
+#pragma unroll
+                    for (int i = 0; i < NI; i++)
+#pragma unroll
+                        for (int k = 0; k < C::NFK; k++) v += ACC(i, j, k, l) * Di[(CI0 + i) * W + rb.kc + k];
+                    atomicAdd(Kj + j * W + rb.lc + l, v);
+                }
+        } else if (sg.vk) {
 #pragma unroll
             for (int i = 0; i < NI; i++)
 #pragma unroll
@@ -496,7 +596,8 @@ __device__ __forceinline__ void jk_thread_products(R* acc, const R* Ix, const R*
 template <class C, typename R, int CI0, int CI1, class Sink>
 __device__ __forceinline__ void jk_thread_pass(const JKSeg& sg, const JKQuartet& q, const double* __restrict__ tab,
                                                const double* ri, const double* rj, const double* rk,
-                                               const double* rl, const Sink& sink) {
+                                               const double* rl, const Sink& sink, const JKFillOut* fo,
+                                               const JKRowBuf& rb) {
     constexpr int NR = C::NROOTS;
     constexpr int NI = CI1 - CI0;
     constexpr int NA = NI * C::NFJ * C::NFK * C::NFL;
@@ -556,29 +657,80 @@ __device__ __forceinline__ void jk_thread_pass(const JKSeg& sg, const JKQuartet&
             }
         }
     }
-    jk_thread_digest<C, R, NI>(sg, q, CI0, acc, sink);
+    if (fo) {  // ERI-tensor fill: the quartet's block goes to the tensor
+        const long long b0 = (long long)(q.i0 + CI0 - fo->off[0]) * fo->st[0] +
+                             (long long)(q.j0 - fo->off[1]) * fo->st[1] + (long long)(q.k0 - fo->off[2]) * fo->st[2] +
+                             (long long)(q.l0 - fo->off[3]) * fo->st[3];
+#pragma unroll
+        for (int i = 0; i < NI; i++)
+#pragma unroll
+            for (int j = 0; j < C::NFJ; j++)
+#pragma unroll
+                for (int k = 0; k < C::NFK; k++)
+#pragma unroll
+                    for (int l = 0; l < C::NFL; l++)
+                        atomicAdd(fo->eri + b0 + i * fo->st[0] + j * fo->st[1] + k * fo->st[2] + l * fo->st[3],
+                                  (double)acc[((i * C::NFJ + j) * C::NFK + k) * C::NFL + l]);
+        return;
+    }
+    jk_thread_digest<C, R, NI>(sg, q, CI0, acc, sink, rb);
 }
 
 
 template <class C, typename R, int PASS, class Sink>
 __device__ __forceinline__ void jk_thread_passes(const JKSeg& sg, const JKQuartet& q, const double* __restrict__ tab,
                                                  const double* ri, const double* rj, const double* rk,
-                                                 const double* rl, const Sink& sink) {
+                                                 const double* rl, const Sink& sink, const JKFillOut* fo,
+                                                 const JKRowBuf& rb) {
     constexpr int CI0 = PASS * C::GI;
     if constexpr (CI0 < C::NFI) {
         constexpr int CI1 = CI0 + C::GI < C::NFI ? CI0 + C::GI : C::NFI;
-        jk_thread_pass<C, R, CI0, CI1>(sg, q, tab, ri, rj, rk, rl, sink);
-        jk_thread_passes<C, R, PASS + 1>(sg, q, tab, ri, rj, rk, rl, sink);
+        jk_thread_pass<C, R, CI0, CI1>(sg, q, tab, ri, rj, rk, rl, sink, fo, rb);
+        jk_thread_passes<C, R, PASS + 1>(sg, q, tab, ri, rj, rk, rl, sink, fo, rb);
     }
 }
 
 template <class C, typename R, class Sink>
 __device__ __forceinline__ void jk_thread_quartet(const JKSeg& sg, const JKQuartet& q, const double* __restrict__ tab,
-                                                  const Sink& sink) {
+                                                  const Sink& sink, const JKFillOut* fo = nullptr,
+                                                  const JKRowBuf& rb = JKRowBuf{nullptr, 0, 0, 0, false}) {
     double ri[3], rj[3], rk[3], rl[3];
     load_pair_centres(sg, q.bij, ri, rj);
     load_pair_centres(sg, q.bkl, rk, rl);
-    jk_thread_passes<C, R, 0>(sg, q, tab, ri, rj, rk, rl, sink);
+    jk_thread_passes<C, R, 0>(sg, q, tab, ri, rj, rk, rl, sink, fo, rb);
+}
+
+// stage the D rows of bra shells i0 (NFI rows) and j0 (NFJ rows) over the
+// columns of the ket groups and clear the K rows (first density)
+template <class C>
+__device__ __forceinline__ void jk_rb_stage(const JKSeg& sg, double* base, int i0, int j0, int lane) {
+    const int W = sg.nk + sg.nl, nao = sg.nao;
+    const int nrow = C::NFI + C::NFJ;
+    const double* D = sg.dm;
+    for (int e = lane; e < nrow * W; e += 32) {
+        const int r = e / W, c = e - r * W;
+        const int a = r < C::NFI ? i0 + r : j0 + (r - C::NFI);
+        const int col = c < sg.nk ? sg.kao0 + c : sg.lao0 + (c - sg.nk);
+        base[e] = __ldg(D + col + (size_t)nao * a);
+        base[nrow * W + e] = 0.;
+    }
+}
+
+// add the K rows to vk with coalesced atomics (transposed orientation:
+// consecutive lanes hold consecutive columns; only V + V^T is used)
+template <class C>
+__device__ __forceinline__ void jk_rb_flush(const JKSeg& sg, double* base, int i0, int j0, int lane) {
+    const int W = sg.nk + sg.nl, nao = sg.nao;
+    const int nrow = C::NFI + C::NFJ;
+    const double* K = base + nrow * W;
+    for (int e = lane; e < nrow * W; e += 32) {
+        const double v = K[e];
+        if (v == 0.) continue;
+        const int r = e / W, c = e - r * W;
+        const int a = r < C::NFI ? i0 + r : j0 + (r - C::NFI);
+        const int col = c < sg.nk ? sg.kao0 + c : sg.lao0 + (c - sg.nk);
+        atomicAdd(sg.vk + col + (size_t)nao * a, v);
+    }
 }
 
 // Resident 128-thread blocks asked of the register allocator (single-segment
@@ -591,32 +743,82 @@ struct JKThreadMinBlocks {
 };
 
 template <class C, typename R, class Src>
-__device__ __forceinline__ void jk_thread_body(const Src& src, double* jk_tab) {
+__device__ __forceinline__ void jk_thread_body(const Src& src, double* jk_tab, const JKFillOut* fo = nullptr) {
     // each warp takes a contiguous chunk of tasks (a multiple of 32); lane i
     // does tasks i, i+32, ... of it, so a warp covers consecutive kl of a row
     const long long total = src.total();
     const int lane = threadIdx.x & 31;
     const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
     const long long wid = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const long long chunk = (((total + nwarps - 1) / nwarps) + 31) & ~31LL;
-    // the grid is sized for the unscreened task count: a block without any
-    // screened task leaves before it loads the Rys table (block-uniform test)
-    if ((long long)blockIdx.x * (blockDim.x >> 5) * chunk >= total) return;
+    unsigned long long* queue = src.queue();
+    const long long chunk = queue ? (long long)src.grab() : (((total + nwarps - 1) / nwarps) + 31) & ~31LL;
+    // static chunks: the grid is sized for the unscreened task count, and a
+    // block without any screened task leaves before it loads the Rys table
+    // (block-uniform test)
+    if (!queue && (long long)blockIdx.x * (blockDim.x >> 5) * chunk >= total) return;
+    if (queue && total == 0) return;
     if constexpr (JKF32Prim<C, R>::value)
         rys_table_to_smem_f<C::NROOTS>(src.first().rys, reinterpret_cast<float*>(jk_tab));
     else
         rys_table_to_smem<C::NROOTS>(src.first().rys, jk_tab);
     __syncthreads();
-    long long t = wid * chunk + lane;
-    const long long tend = min(total, (wid + 1) * chunk);
-    if (t >= tend) return;
-    typename Src::Cursor cur;
-    cur.init(src, t);
-    for (; t < tend; t += 32) {
-        int row, col;
-        const JKSeg& sg = cur.seek(src, t, row, col);
-        JKQuartet q = jk_quartet_at(sg, row, col);
-        jk_thread_quartet<C, R>(sg, q, jk_tab, jk_sink_global(sg));
+    long long c0 = wid * chunk;
+    for (;;) {
+        if (queue) {
+            unsigned long long g = 0;
+            if (lane == 0) g = atomicAdd(queue, (unsigned long long)chunk);
+            c0 = (long long)__shfl_sync(0xffffffffu, g, 0);
+        }
+        if (c0 >= total) break;
+        long long t = c0 + lane;
+        const long long tend = min(total, c0 + chunk);
+        // row buffers (single segment, enabled by the launcher)
+        const JKSeg& sg0 = src.first();
+        const bool rbon = Src::ROWBUF && !fo && sg0.rb_words > 0;
+        double* rbase = jk_tab + RysS<C::NROOTS>::WORDS + (threadIdx.x >> 5) * (rbon ? sg0.rb_words : 0);
+        int rb_bij = -1, rb_skip = -1, rb_i0 = 0, rb_j0 = 0;
+        if (t < tend) {
+            typename Src::Cursor cur;
+            cur.init(src, t);
+            for (; t < tend; t += 32) {
+                int row, col;
+                const JKSeg& sg = cur.seek(src, t, row, col);
+                JKQuartet q = jk_quartet_at(sg, row, col);
+                if (fo) q.norm = JK_FAC;  // the fill has no 1/2 on the ij == kl diagonal
+                JKRowBuf rb{rbase, sg.nk + sg.nl, q.k0 - sg.kao0, sg.nk + q.l0 - sg.lao0, false};
+                if (rbon) {
+                    const unsigned am = __activemask();
+                    if (am == 0xffffffffu) {
+                        const int b0 = __shfl_sync(am, q.bij, 0);
+                        if (b0 != rb_bij && b0 != rb_skip) {
+                            __syncwarp();
+                            if (rb_bij >= 0) jk_rb_flush<C>(sg, rbase, rb_i0, rb_j0, lane);
+                            // tasks of lane 0's row left in this chunk
+                            const long long rem = __shfl_sync(am, min(cur.row_end(), tend) - t, 0);
+                            if (rem >= JK_RB_MIN_TASKS) {
+                                rb_i0 = __shfl_sync(am, q.i0, 0);
+                                rb_j0 = __shfl_sync(am, q.j0, 0);
+                                __syncwarp();
+                                jk_rb_stage<C>(sg, rbase, rb_i0, rb_j0, lane);
+                                rb_bij = b0;
+                                rb_skip = -1;
+                            } else {
+                                rb_bij = -1;
+                                rb_skip = b0;
+                            }
+                            __syncwarp();
+                        }
+                        rb.on = rb_bij >= 0 && q.bij == rb_bij;
+                    }
+                }
+                jk_thread_quartet<C, R>(sg, q, jk_tab, jk_sink_global(sg), fo, rb);
+            }
+        }
+        if (rbon && rb_bij >= 0) {
+            __syncwarp();
+            jk_rb_flush<C>(sg0, rbase, rb_i0, rb_j0, lane);
+        }
+        if (!queue) break;
     }
 }
 
@@ -628,12 +830,23 @@ __global__ void __launch_bounds__(128, (JKThreadMinBlocks<C, R>::value)) jk_thre
     jk_thread_body<C, R>(src, jk_tab);
 }
 
+// ERI-tensor fill with the thread kernel's register recursion (FP64)
+template <class C>
+__global__ void __launch_bounds__(128, C::MINB) jk_thread_fill_kernel(const __grid_constant__ JKSeg sg,
+                                                                      const long long* __restrict__ task0,
+                                                                      const __grid_constant__ JKFillOut out) {
+    extern __shared__ __align__(16) double jk_tab[];
+    JKOneSeg src{sg, task0};
+    jk_thread_body<C, double>(src, jk_tab, &out);
+}
+
 template <class C, typename R>
 __global__ void __launch_bounds__(128, C::MINB) jk_thread_kernel_batch(const JKSeg* __restrict__ segs,
                                                                        const long long* __restrict__ segt,
-                                                                       int nseg) {
+                                                                       int nseg, unsigned long long* queue,
+                                                                       int grab) {
     extern __shared__ __align__(16) double jk_tab[];
-    JKSegTable src{segs, segt, nseg};
+    JKSegTable src{segs, segt, nseg, queue, grab};
     jk_thread_body<C, R>(src, jk_tab);
 }
 
@@ -791,7 +1004,7 @@ __host__ __device__ constexpr size_t jk_team_smem() {
 }
 
 template <class C, typename R, class Src>
-__device__ __forceinline__ void jk_team_body(const Src& src) {
+__device__ __forceinline__ void jk_team_body(const Src& src, const JKFillOut* fo = nullptr) {
     using S = JKTeamShape<C>;
     using L = JKTeamLayout<C, R>;
     constexpr int T = C::T, NR = C::NROOTS;
@@ -809,8 +1022,12 @@ __device__ __forceinline__ void jk_team_body(const Src& src) {
     // team has no screened task leaves before it loads the Rys table.
     const long long total = src.total();
     const long long nteams = (long long)gridDim.x * S::QPB;
-    const long long chunk = (total + nteams - 1) / nteams;
-    if ((long long)blockIdx.x * S::QPB * chunk >= total) return;
+    unsigned long long* queue = src.queue();
+    // tasks per team and round: the whole static chunk, or one grab of the
+    // persistent mode (a block takes QPB grabs at once)
+    const long long chunk = queue ? (long long)src.grab() : (total + nteams - 1) / nteams;
+    if (!queue && (long long)blockIdx.x * S::QPB * chunk >= total) return;
+    if (queue && total == 0) return;
     // FP32 quartets at low order: float prefactors, nodes and weights (the
     // table copy in shared memory is then single precision)
     constexpr bool F32P = JKF32Prim<C, R>::value && S::SMEM_TAB;
@@ -835,8 +1052,17 @@ __device__ __forceinline__ void jk_team_body(const Src& src) {
 
     __syncthreads();
     const int nprim_ij = sg0.nprim_ij, nprim_kl = sg0.nprim_kl;  // uniform within a launch
-    const long long tid = (long long)blockIdx.x * S::QPB + team;
-    const long long tbeg = tid * chunk, tend = min(total, tbeg + chunk);
+    __shared__ long long s_grab;
+    long long bbase = (long long)blockIdx.x * S::QPB * chunk;
+    for (;;) {
+    if (queue) {
+        __syncthreads();  // the previous round's readers of s_grab are done
+        if (threadIdx.x == 0) s_grab = (long long)atomicAdd(queue, (unsigned long long)(chunk * S::QPB));
+        __syncthreads();
+        bbase = s_grab;
+        if (bbase >= total) break;  // block-uniform
+    }
+    const long long tbeg = bbase + team * chunk, tend = min(total, tbeg + chunk);
     typename Src::Cursor cur;
     if (tbeg < tend) cur.init(src, tbeg);
     for (long long it = 0; it < chunk; it++) {
@@ -849,6 +1075,7 @@ __device__ __forceinline__ void jk_team_body(const Src& src) {
             int row, col;
             sgp = &cur.seek(src, t, row, col);
             q = jk_quartet_at(*sgp, row, col);
+            if (fo) q.norm = JK_FAC;  // the fill has no 1/2 on the ij == kl diagonal
         }
         const JKSeg& sg = *sgp;
         if (active) {
@@ -933,6 +1160,31 @@ __device__ __forceinline__ void jk_team_body(const Src& src) {
             }
         }
 
+        if (fo) {  // ERI-tensor fill: each thread writes its owned components
+            if (active) {
+                const long long b0 = (long long)(q.i0 + ci - fo->off[0]) * fo->st[0] +
+                                     (long long)(q.j0 + cj - fo->off[1]) * fo->st[1] +
+                                     (long long)(q.k0 - fo->off[2]) * fo->st[2] +
+                                     (long long)(q.l0 - fo->off[3]) * fo->st[3];
+                if (C::P == 1) {
+#pragma unroll
+                    for (int j = 0; j < C::NFJ; j++)
+#pragma unroll
+                        for (int k = 0; k < C::NFK; k++)
+#pragma unroll
+                            for (int l = 0; l < C::NFL; l++)
+                                atomicAdd(fo->eri + b0 + j * fo->st[1] + k * fo->st[2] + l * fo->st[3],
+                                          (double)acc[(j * C::NFK + k) * C::NFL + l]);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < C::NFK; k++)
+#pragma unroll
+                        for (int l = 0; l < C::NFL; l++)
+                            atomicAdd(fo->eri + b0 + k * fo->st[2] + l * fo->st[3], (double)acc[k * C::NFL + l]);
+                }
+            }
+            continue;
+        }
         // ---- digestion ----
         // Outputs a thread owns completely go to buf; the others are written as
         // per-thread partials (no shared atomics), summed by the team after a
@@ -1136,6 +1388,8 @@ __device__ __forceinline__ void jk_team_body(const Src& src) {
             __syncthreads();
         }
     }
+    if (!queue) break;
+    }
 }
 template <class C, typename R>
 __global__ void jk_team_kernel(const __grid_constant__ JKSeg sg, const long long* __restrict__ task0) {
@@ -1143,9 +1397,18 @@ __global__ void jk_team_kernel(const __grid_constant__ JKSeg sg, const long long
     jk_team_body<C, R>(src);
 }
 
+// ERI-tensor fill with the team kernel's recursion (FP64)
+template <class C>
+__global__ void jk_team_fill_kernel(const __grid_constant__ JKSeg sg, const long long* __restrict__ task0,
+                                    const __grid_constant__ JKFillOut out) {
+    JKOneSeg src{sg, task0};
+    jk_team_body<C, double>(src, &out);
+}
+
 template <class C, typename R>
-__global__ void jk_team_kernel_batch(const JKSeg* __restrict__ segs, const long long* __restrict__ segt, int nseg) {
-    JKSegTable src{segs, segt, nseg};
+__global__ void jk_team_kernel_batch(const JKSeg* __restrict__ segs, const long long* __restrict__ segt, int nseg,
+                                     unsigned long long* queue, int grab) {
+    JKSegTable src{segs, segt, nseg, queue, grab};
     jk_team_body<C, R>(src);
 }
 #undef DM

@@ -19,7 +19,9 @@ class JKOpts(ctypes.Structure):
                 ('nbins', ctypes.c_int),
                 ('prescreen', ctypes.c_int),
                 ('fp32_cutoff', ctypes.c_double),
-                ('reserved', ctypes.c_int * 8)]
+                ('shard', ctypes.c_int),
+                ('nshards', ctypes.c_int),
+                ('reserved', ctypes.c_int * 6)]
 
 
 _LIB = None
@@ -70,6 +72,12 @@ _SIGNATURES = {
     'jk_batch_get_jk': [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                         ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
+    'jk_batch_tune': [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                      ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                      ctypes.c_char_p, ctypes.c_void_p],
+    'jk_batch_info': [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    'jk_shard_plan': [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                      ctypes.c_void_p],
     'jk_last_error': [],
 }
 

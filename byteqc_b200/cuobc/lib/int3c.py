@@ -67,15 +67,15 @@ class VHFOpt3c:
 
     def build(self, cutoff=1e-13, group_size=None, aux_group_size=None,
               diag_block_with_triu=True, gpus=None):
-        from byteqc_b200.cuobc.scf.hf import LMAX_ON_GPU
+        from byteqc_b200.cuobc.scf.hf import LMAX_ENGINE
         lib = _lib.load_library()
         smol, coeff, counts = sort_mol(self.mol0, group_size)
         saux, auxcoeff, acounts = sort_mol(self.auxmol0, aux_group_size)
         tot = gmole.conc_mol(smol, gmole.conc_mol(make_fake_mol(), saux))
         lmax = int(tot._bas[:, gmole.ANG_OF].max())
-        if lmax > LMAX_ON_GPU:
+        if lmax > LMAX_ENGINE:
             raise NotImplementedError('shells with l=%d: this engine handles '
-                                      'l <= %d' % (lmax, LMAX_ON_GPU))
+                                      'l <= %d' % (lmax, LMAX_ENGINE))
         groups = np.concatenate([counts, [1], acounts]).astype(np.int64)
         offsets = np.append(0, np.cumsum(groups)).astype(np.int32)
         handle = ctypes.c_void_p()

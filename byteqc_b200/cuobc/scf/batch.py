@@ -4,8 +4,12 @@
 ``get_jk(dms)`` returns [(vj, vk), ...] for all molecules from a single
 sequence of launches (one per class shared by the molecules), and
 ``capture(dms)`` / ``replay()`` record that sequence in a CUDA graph so an SCF
-iteration of the whole batch is one graph launch.  Densities and results use
-the layout of the single-molecule ``get_jk`` (``cuobc/scf/hf.py:53-227``).
+iteration of the whole batch is one graph launch.  ``tune(dms)`` runs the
+engine's autotuner (``jk_batch_tune``): every class launch of the batch is
+timed in its candidate shapes (static chunks, or persistent grids taking
+chunks from a device counter) and the fastest is kept, optionally through a
+cache file.  Densities and results use the layout of the single-molecule
+``get_jk`` (``cuobc/scf/hf.py:53-227``).
 """
 import ctypes
 
@@ -104,6 +108,58 @@ class JKBatch:
         self._run(n_dm, with_j, with_k, self._opts(prescreen, nbins,
                                                    fp32_cutoff))
         return self._results(shapes, with_j, with_k, out)
+
+    # -- autotuner -----------------------------------------------------------
+    def tune(self, dms, prescreen=True, nbins=None, fp32_cutoff=None,
+             cache=None):
+        """Choose the launch shape of every class launch of the batch by
+        timing the candidates on these densities (FP64 part, and the FP32
+        part when ``fp32_cutoff`` > 0).  ``cache``: path of a text file of
+        earlier choices, read first and rewritten.  A captured graph is
+        dropped (it holds the old shapes).  Returns ``info()``."""
+        torch = self.torch
+        n_dm, _ = self._load(dms)
+        _, bdm, _, _ = self._buffers
+        w, vj, vk = [], [], []
+        for b, op in zip(bdm, self.opts):
+            C = op.coeff_dev
+            w.append(torch.stack([C @ b[d] @ C.T for d in range(n_dm)])
+                     .contiguous())
+            vj.append(torch.zeros_like(w[-1]))
+            vk.append(torch.zeros_like(w[-1]))
+        o = self._opts(prescreen, nbins, fp32_cutoff)
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        _lib.check(self.lib.jk_batch_tune(
+            self.handle, _ptrs([x.data_ptr() for x in w]),
+            _ptrs([x.data_ptr() for x in vj]),
+            _ptrs([x.data_ptr() for x in vk]), n_dm, ctypes.byref(o),
+            cache.encode() if cache else None, stream), 'jk_batch_tune')
+        self._graph = None
+        return self.info()
+
+    def info(self):
+        """Launch shape of every class launch: class index, primitive
+        counts (-1: any), task bound, and per part (FP64, FP32) the grab
+        (0: static chunks), grid multiple, tuned time (ms, None if not
+        tuned) and segment count."""
+        n = ctypes.c_int()
+        _lib.check(self.lib.jk_batch_info(self.handle, ctypes.byref(n), None),
+                   'jk_batch_info')
+        out = np.zeros((max(n.value, 1), 12), dtype=np.int32)
+        _lib.check(self.lib.jk_batch_info(self.handle, ctypes.byref(n),
+                                          out.ctypes.data), 'jk_batch_info')
+        res = []
+        for r in out[:n.value]:
+            parts = []
+            for p in range(2):
+                g, gm, us, ns = (int(v) for v in r[4 + 4 * p:8 + 4 * p])
+                parts.append({'grab': g, 'grid_mul': gm,
+                              'ms': us / 1e3 if us >= 0 else None,
+                              'segments': ns})
+            res.append({'class': int(r[0]), 'np_ij': int(r[1]),
+                        'np_kl': int(r[2]), 'tasks': int(r[3]),
+                        'fp64': parts[0], 'fp32': parts[1]})
+        return res
 
     # -- CUDA graph of one batched build ----------------------------------
     def capture(self, dms, with_j=True, with_k=True, prescreen=True,

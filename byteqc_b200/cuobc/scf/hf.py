@@ -23,7 +23,10 @@ import numpy as np
 from byteqc_b200.cuobc import lib as _lib
 from byteqc_b200.gto import mole as gmole
 
-LMAX_ON_GPU = 5  # h functions, as the reference's GPU kernels
+LMAX_ON_GPU = 5  # h functions: the reference's GPU limit (group splitting)
+# Shells up to i (l = 6) run on the GPU here; the reference hands quartets
+# with an i shell to PySCF on the CPU (cuobc/scf/hf.py:185-218).
+LMAX_ENGINE = 6
 ANGULAR = 'spdfghik'
 
 
@@ -134,10 +137,10 @@ class _VHFOpt:
             l_ctrs, return_inverse=True, return_counts=True, axis=0)
         inv_idx = np.asarray(inv_idx).ravel()
         lmax = int(uniq_l_ctr[:, 0].max())
-        if lmax > LMAX_ON_GPU:
+        if lmax > LMAX_ENGINE:
             raise NotImplementedError(
                 'shells with l=%d: this engine handles l <= %d'
-                % (lmax, LMAX_ON_GPU))
+                % (lmax, LMAX_ENGINE))
         if group_size is not None:
             uniq_l_ctr, l_ctr_counts = _split_l_ctr_groups(
                 uniq_l_ctr, l_ctr_counts, group_size)
@@ -208,13 +211,22 @@ class _VHFOpt:
 
 def get_jk(mol, dm, hermi=1, vhfopt=None, with_j=True, with_k=True,
            omega=None, verbose=None, group_size=None, gpus=None,
-           prescreen=True, nbins=None, out='host', fp32_cutoff=None):
+           prescreen=True, nbins=None, out='host', fp32_cutoff=None,
+           group=None):
     """Coulomb and exchange matrices of the density matrices ``dm``.
 
     ``fp32_cutoff``: mixed precision -- contracted quartets whose screened
     bound q_ij q_kl max|D| is below it run the Rys recursion and products in
     FP32 (roots, weights, prefactors and all J/K accumulation stay FP64);
-    None or 0 keeps everything in FP64 (the reference's arithmetic)."""
+    None or 0 keeps everything in FP64 (the reference's arithmetic).
+
+    ``group``: a ``torch.distributed`` process group, one rank per GPU (the
+    reference's multi-GPU task farm, cuobc/scf/hf.py:147-169 with
+    lib/multigpu.py:136-329): every rank builds its share of the class
+    quartets (``jk_shard_plan`` on their cost, the same plan on every rank)
+    and the partial J and K are summed by one all-reduce each, so every rank
+    returns the full result.  Every rank of the group must call with the
+    same molecule and density."""
     if hermi != 1:
         raise NotImplementedError(
             'JK-builder only supports hermitian density matrix')
@@ -239,10 +251,19 @@ def get_jk(mol, dm, hermi=1, vhfopt=None, with_j=True, with_k=True,
     opts.nbins = nbins if nbins is not None else vhfopt.default_nbins()
     opts.prescreen = int(bool(prescreen))
     opts.fp32_cutoff = float(fp32_cutoff or 0.)
+    if group is not None:
+        import torch.distributed as dist
+        opts.shard = dist.get_rank(group)
+        opts.nshards = dist.get_world_size(group)
     _lib.check(lib.jk_get_jk(
         vhfopt.handle, vhfopt.coeff_dev.data_ptr(), nao0, d.data_ptr(), n_dm,
         vj.data_ptr() if with_j else None, vk.data_ptr() if with_k else None,
         ctypes.byref(opts), _stream_ptr(torch)), 'jk_get_jk')
+    if group is not None and opts.nshards > 1:
+        import torch.distributed as dist
+        for v in (vj, vk):
+            if v is not None:
+                dist.all_reduce(v, group=group)
     res = []
     for v in (vj, vk):
         if v is None:

@@ -1,24 +1,28 @@
 """Continuous-batching J/K server: many SCF calculations share the GPU.
 
 Requests (a molecule, optionally a starting density) arrive over time; each
-runs ``n_iter`` SCF iterations whose J/K builds the server executes.  The
-scheduler loop
+runs ``n_iter`` SCF iterations (or fewer, once its energy change falls below
+``conv_tol``) whose J/K builds the server executes.  The scheduler loop
 
-* admits waiting requests while a slot is free and their estimated device
-  footprint fits the HBM budget (setup -- Schwarz screening and pair cache --
-  runs at admission and stays on the device with the request's density, Fock
-  history and orbitals until it finishes);
+* admits waiting requests while a slot is free and their device footprint,
+  bounded from the basis sizes before anything is allocated, fits the HBM
+  budget (setup -- Schwarz screening and pair cache -- then runs at admission
+  and stays on the device with the request's density, Fock history and
+  orbitals until it finishes; the exact footprint replaces the bound);
 * runs ONE batched J/K pass for all admitted requests (each request's
   iteration k), so requests that arrived at different times overlap on the
-  device;
+  device; the engine batch is kept while the set of active requests does
+  not change and rebuilt when one joins or leaves;
 * advances every request's SCF state (Fock matrix, DIIS, eigensolver, all on
   the device) and retires finished requests, freeing their slot and memory.
 
-Per-build latency (issue to completion of one request's J/K build) and
-per-request latency (arrival to last iteration) are recorded; ``stats()``
-reports their p50/p99 and the builds/s.  The result of a request does not
-depend on what it was batched with: every J/K build is the same computation
-with the same screening as a build of that molecule alone.
+Recorded per request: the latency of each of its J/K builds (issue to
+completion of the batched pass that carries it: all builds of a pass
+complete together), of each of its iterations (step start to the end of
+its own SCF update), and of the whole request (arrival to last iteration);
+``stats()`` reports their p50/p99 and the builds/s.  The result of a request
+does not depend on what it was batched with: every J/K build is the same
+computation with the same screening as a build of that molecule alone.
 """
 import collections
 import time
@@ -27,6 +31,24 @@ import numpy as np
 
 from byteqc_b200.cuobc.scf import hf
 from byteqc_b200.cuobc.scf.batch import JKBatch
+
+
+def footprint_bound_bytes(mol):
+    """Upper bound of footprint_bytes(opt) from the basis alone (no device
+    work, nothing allocated): every shell pair counted as kept by the
+    Schwarz screen."""
+    pmol, coeff = hf.basis_seg_contraction(mol)
+    bas = pmol._bas
+    nbas = int(bas.shape[0])
+    ls = bas[:, 1]
+    nps = bas[:, 2].astype(np.int64)
+    nao = int(((ls + 1) * (ls + 2) // 2).sum())
+    nao0 = coeff.shape[1]
+    npairs = nbas * (nbas + 1) // 2
+    nprim = int((nps.sum() ** 2 + (nps ** 2).sum()) // 2)
+    words = (nbas * nbas + 4 * npairs + 6 * nprim + 6 * npairs
+             + 6 * nao * nao + nao * nao0 + 16 * nao0 * nao0)
+    return 8 * words
 
 
 def footprint_bytes(opt):
@@ -45,16 +67,19 @@ def footprint_bytes(opt):
 
 
 class _Request:
-    def __init__(self, rid, mol, arrival, n_iter, dm0):
+    def __init__(self, rid, mol, arrival, n_iter, dm0, conv_tol):
         self.rid = rid
         self.mol = mol
         self.arrival = arrival
         self.n_iter = n_iter
         self.dm0 = dm0
+        self.conv_tol = conv_tol
         self.iter = 0
         self.energies = []
         self.build_lat = []
+        self.iter_lat = []
         self.done_time = None
+        self.converged = False
 
 
 class _SCFState:
@@ -106,13 +131,14 @@ class _SCFState:
 
 class JKServer:
     def __init__(self, hbm_budget_bytes=40 << 30, max_slots=64,
-                 fp32_cutoff=None, n_iter=15, cutoff=1e-13):
+                 fp32_cutoff=None, n_iter=15, cutoff=1e-13, conv_tol=None):
         self.torch = hf._torch()
         self.budget = hbm_budget_bytes
         self.max_slots = max_slots
         self.fp32_cutoff = fp32_cutoff
         self.n_iter = n_iter
         self.cutoff = cutoff
+        self.conv_tol = conv_tol
         self.waiting = collections.deque()
         self.active = []  # (request, opt, state, bytes)
         self.finished = []
@@ -120,29 +146,42 @@ class JKServer:
         self.builds = 0
         self.steps = 0
         self._next_id = 0
+        self._batch = None
+        self._batch_ids = None
+        self.batch_builds = 0  # engine batches created
 
     def submit(self, mol, arrival=None, dm0=None, n_iter=None):
         rid = self._next_id
         self._next_id += 1
         self.waiting.append(_Request(rid, mol, time.perf_counter() if arrival is None else arrival,
-                                     n_iter or self.n_iter, dm0))
+                                     n_iter or self.n_iter, dm0, self.conv_tol))
         return rid
 
     def _admit(self):
         while self.waiting and len(self.active) < self.max_slots:
             req = self.waiting[0]
+            bound = footprint_bound_bytes(req.mol)
+            if bound > self.budget:
+                raise MemoryError('request %d may need %d bytes, over the '
+                                  'budget' % (req.rid, bound))
+            if self.active and self.used + bound > self.budget:
+                break
+            self.waiting.popleft()
             opt = hf._VHFOpt(req.mol).build(self.cutoff)
             need = footprint_bytes(opt)
-            if self.active and self.used + need > self.budget:
-                opt.clear()
-                break
-            if need > self.budget:
-                opt.clear()
-                raise MemoryError('request %d needs %d bytes, over the budget'
-                                  % (req.rid, need))
-            self.waiting.popleft()
             self.active.append((req, opt, _SCFState(req, opt, self.torch), need))
             self.used += need
+
+    def _engine_batch(self):
+        ids = tuple(a[0].rid for a in self.active)
+        if ids != self._batch_ids:
+            if self._batch is not None:
+                self._batch.close()
+            self._batch = JKBatch([a[0].mol for a in self.active],
+                                  vhfopts=[a[1] for a in self.active])
+            self._batch_ids = ids
+            self.batch_builds += 1
+        return self._batch
 
     def step(self):
         """Admit, run one batched J/K pass for every active request, advance
@@ -152,8 +191,8 @@ class JKServer:
         self._admit()
         if not self.active:
             return 0
-        batch = JKBatch([a[0].mol for a in self.active],
-                        vhfopts=[a[1] for a in self.active])
+        t0 = time.perf_counter()
+        batch = self._engine_batch()
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         ev0.record()
@@ -162,14 +201,17 @@ class JKServer:
         ev1.record()
         ev1.synchronize()
         lat = ev0.elapsed_time(ev1) * 1e-3
-        batch.close()
         still = []
-        now = time.perf_counter()
         for (req, opt, st, nbytes), (vj, vk) in zip(self.active, res):
             req.energies.append(st.update(vj, vk))
+            torch.cuda.current_stream().synchronize()
             req.build_lat.append(lat)
+            req.iter_lat.append(time.perf_counter() - t0)
             req.iter += 1
-            if req.iter >= req.n_iter:
+            conv = (req.conv_tol is not None and len(req.energies) > 1 and
+                    abs(req.energies[-1] - req.energies[-2]) < req.conv_tol)
+            if conv or req.iter >= req.n_iter:
+                req.converged = conv
                 req.done_time = time.perf_counter()
                 req.dm_final = st.dm
                 self.finished.append(req)
@@ -177,10 +219,12 @@ class JKServer:
                 opt.clear()
             else:
                 still.append((req, opt, st, nbytes))
+        if len(still) != len(self.active) and self._batch is not None:
+            self._batch.close()  # its molecules change: rebuilt next step
+            self._batch, self._batch_ids = None, None
         self.active = still
         self.builds += len(res)
         self.steps += 1
-        del now
         return len(res)
 
     def run_until_empty(self):
@@ -189,11 +233,15 @@ class JKServer:
 
     def stats(self):
         lat = np.array([x for r in self.finished for x in r.build_lat])
+        itl = np.array([x for r in self.finished for x in r.iter_lat])
         req = np.array([r.done_time - r.arrival for r in self.finished])
-        out = {'requests': len(self.finished), 'builds': int(lat.size)}
+        out = {'requests': len(self.finished), 'builds': int(lat.size),
+               'engine_batches': self.batch_builds, 'steps': self.steps}
         if lat.size:
             out.update(build_p50_ms=float(np.percentile(lat, 50) * 1e3),
-                       build_p99_ms=float(np.percentile(lat, 99) * 1e3))
+                       build_p99_ms=float(np.percentile(lat, 99) * 1e3),
+                       iteration_p50_ms=float(np.percentile(itl, 50) * 1e3),
+                       iteration_p99_ms=float(np.percentile(itl, 99) * 1e3))
         if req.size:
             out.update(request_p50_s=float(np.percentile(req, 50)),
                        request_p99_s=float(np.percentile(req, 99)))

@@ -38,7 +38,12 @@ typedef struct {
     int prescreen;         /* class-level density screen on/off (hf.py:139)   */
     double fp32_cutoff;    /* mixed precision: FP32 recursion below this bound;
                               0 disables                                       */
-    int reserved[8];
+    int shard;             /* sharded builds (one GPU per rank): this rank's  */
+    int nshards;           /* share of nshards (0 or 1: the whole build); the
+                              class quartets are split by jk_shard_plan on
+                              their cost, and the partial J/K of the ranks
+                              sum to the full J/K (all-reduce them)            */
+    int reserved[6];
 } jk_opts_t;
 
 /*
@@ -132,6 +137,17 @@ int jk_build(jk_basis_t *basis, const double *dm, int n_dm, double *vj, double *
              void *stream);
 
 /*
+ * Split of n weighted tasks over nshards owners (the class quartets of a
+ * sharded build, weighted by their unscreened work): longest first, each to
+ * the owner with the least work so far (ties: lower index), so every rank
+ * computes the same plan.  owner[i] in [0, nshards).  Host code only.  The
+ * reference farms class pairs to GPUs dynamically from a Python task loop
+ * (cuobc/lib/multigpu.py:136-329, cuobc/scf/hf.py:165-169); a static
+ * plan needs no coordination between ranks.
+ */
+int jk_shard_plan(const double *cost, int n, int nshards, int *owner);
+
+/*
  * Full J/K in the caller's basis: dms = C D C^T, jk_build, then
  * J = 2 C^T (V + V^T) C and K = C^T (V + V^T) C (cuobc/scf/hf.py:67-181).
  * coeff: device (nao, nao0) row-major (the working basis -> caller basis map);
@@ -145,9 +161,12 @@ int jk_get_jk(jk_basis_t *basis, const double *coeff, int nao0, const double *dm
  * Batched builds over many molecules (one jk_basis each, same device).  No
  * single reference counterpart: the reference builds one molecule at a time
  * through the task loop of get_jk (cuobc/scf/hf.py:111-166); a batch runs
- * the class quartets of all molecules that share a class (angular momenta
- * and primitive counts) as one launch, with the same screening decisions as
- * jk_build for each molecule.
+ * the class quartets of all molecules that share a class (angular momenta,
+ * and primitive counts for the team kernels) as one launch, largest
+ * molecules' work first, with the same screening decisions as jk_build for
+ * each molecule.  Each launch takes static chunks or runs persistent (a grid
+ * of the device's resident capacity taking chunks from a device counter),
+ * as jk_batch_tune chose; untuned batches use static chunks.
  */
 int jk_batch_create(jk_basis_t *const *bases, int nmol, jk_batch_t **out);
 int jk_batch_destroy(jk_batch_t *batch);
@@ -159,6 +178,26 @@ int jk_batch_destroy(jk_batch_t *batch);
  * asynchronous. */
 int jk_batch_build(jk_batch_t *batch, const double *const *dms, double *const *vjs, double *const *vks, int n_dm,
                    const jk_opts_t *opts, void *stream);
+
+/* Autotuner of the batch's launch shapes (no reference counterpart: the
+ * reference launches a fixed 256-thread shape per class pair and bin,
+ * cuobc/lib/gint/gint.h:52).  Times every candidate shape of every class
+ * launch of the batch (static chunks; persistent at one or two resident
+ * grids with three grab sizes) with CUDA events on `stream`, after the
+ * bookkeeping of a real build with these arguments (same contract as
+ * jk_batch_build), and keeps the fastest.  cache_path (may be NULL): a text
+ * file of earlier choices per (class, primitive counts, part, log2 task
+ * count), read first (those launches are not timed again) and rewritten
+ * with all choices.  The timing runs accumulate into vjs/vks, which are
+ * zeroed before return; the call synchronises `stream`. */
+int jk_batch_tune(jk_batch_t *batch, const double *const *dms, double *const *vjs, double *const *vks, int n_dm,
+                  const jk_opts_t *opts, const char *cache_path, void *stream);
+
+/* Launch shapes of the batch: *nkeys set; if out is not NULL, 12 ints per
+ * key: class index, primitive counts of bra and ket pairs (-1: any), task
+ * bound, then for the FP64 and FP32 parts: grab (0: static), grid multiple,
+ * tuned time in microseconds (-1: not tuned), segments. */
+int jk_batch_info(const jk_batch_t *batch, int *nkeys, int *out);
 
 /* Full J/K of every molecule in its own basis (the jk_get_jk contract per
  * molecule): coeffs[m] device (nao_m, nao0s[m]); dm0s[m], vj0s[m], vk0s[m]

@@ -28,7 +28,8 @@ import oracle
 from byteqc_b200.gto import mole as gmole  # libcint slot indices only
 from oracle import gto_oracle
 
-LMAX_ON_GPU = 5
+LMAX_ON_GPU = 5  # the reference's GPU limit, used by the group split
+LMAX_ORACLE = 6
 
 
 def basis_seg_contraction(mol):
@@ -125,8 +126,11 @@ class VHFOpt:
             l_ctrs, return_index=True, return_inverse=True,
             return_counts=True, axis=0)
         inv_idx = np.asarray(inv_idx).ravel()
-        if uniq_l_ctr[:, 0].max() > LMAX_ON_GPU:
-            raise NotImplementedError('l > 5 shells')
+        # the reference computes quartets with a shell above h on the CPU
+        # through PySCF (hf.py:185-218); the oracle keeps them in the same
+        # screened loop as the rest, up to i shells
+        if uniq_l_ctr[:, 0].max() > LMAX_ORACLE:
+            raise NotImplementedError('l > 6 shells')
         if group_size is not None:
             uniq_l_ctr, l_ctr_counts = _split_l_ctr_groups(
                 uniq_l_ctr, l_ctr_counts, group_size)

@@ -45,8 +45,8 @@
 #define NPRIM_OF 2
 #define PTR_EXP 5
 #define PTR_COEFF 6
-#define LMAX 5
-#define NF_MAX 21
+#define LMAX 6
+#define NF_MAX 28
 
 static double common_fac_sp(int l) {
     if (l == 0) return 0.282094791773878143;

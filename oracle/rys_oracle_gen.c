@@ -162,7 +162,7 @@ static void hermite_limit(int n, qf *r, qf *hw) {
 int main(int argc, char **argv) {
     if (argc < 3) return 2;
     int nmax = atoi(argv[1]);
-    if (nmax < 1 || nmax > 12) return 2;
+    if (nmax < 1 || nmax > NMAXO) return 2;
     gauss_legendre();
     FILE *fo = fopen(argv[2], "w");
     if (!fo) return 1;

@@ -121,3 +121,76 @@ def test_batch_molecules_vs_oracle():
         assert abs(res[m][0] - rj).max() <= 1e-10, m
         assert abs(res[m][1] - rk).max() <= 1e-10, m
     batch.close()
+
+
+def test_batch_tune_keeps_results_and_cache(tmp_path):
+    """The autotuner picks a launch shape per class launch (static chunks or
+    a persistent grid with a device work counter); the batched J/K are the
+    same before and after tuning, in FP64 and in the mixed mode, and a second
+    tuning from the cache file times nothing again."""
+    from byteqc_b200.cuobc.scf.batch import JKBatch
+    mols = _mols()
+    dms = _dms(mols, seed=9)
+    batch = JKBatch(mols)
+    ref = batch.get_jk(dms)
+    ref32 = batch.get_jk(dms, fp32_cutoff=1e-6)
+    cache = str(tmp_path / 'tune.txt')
+    info = batch.tune(dms, fp32_cutoff=1e-6, cache=cache)
+    assert info and all(k['fp64']['ms'] is not None for k in info)
+    assert all(k['fp32']['ms'] is not None for k in info)
+    got = batch.get_jk(dms)
+    got32 = batch.get_jk(dms, fp32_cutoff=1e-6)
+    for (aj, ak), (bj, bk) in zip(ref, got):
+        assert abs(aj - bj).max() <= 1e-10
+        assert abs(ak - bk).max() <= 1e-10
+    for (aj, ak), (bj, bk) in zip(ref32, got32):
+        assert abs(aj - bj).max() <= 1e-10
+        assert abs(ak - bk).max() <= 1e-10
+    # every persistent shape also gives the same result in a captured graph
+    batch.capture(dms)
+    rep = batch.replay(dms)
+    for (aj, ak), (bj, bk) in zip(ref, rep):
+        assert abs(aj - bj).max() <= 1e-10
+        assert abs(ak - bk).max() <= 1e-10
+    lines = open(cache).read().splitlines()
+    assert len(lines) > 1
+    b2 = JKBatch(mols, vhfopts=batch.opts)
+    info2 = b2.tune(dms, fp32_cutoff=1e-6, cache=cache)
+    shapes = {(k['class'], k['np_ij'], k['np_kl']): (k['fp64']['grab'],
+              k['fp64']['grid_mul']) for k in info}
+    for k in info2:
+        assert shapes[(k['class'], k['np_ij'], k['np_kl'])] == (
+            k['fp64']['grab'], k['fp64']['grid_mul'])
+    b2.close()
+    batch.close()
+
+
+def test_batch_persistent_shapes_match_static():
+    """Every persistent launch shape gives the static result: the batch's
+    class launches forced to each candidate grab size (through a cache file
+    written by hand) on molecules of uneven size."""
+    import os
+    import tempfile
+    from byteqc_b200.cuobc.scf.batch import JKBatch
+    mols = _mols()
+    dms = _dms(mols, seed=10)
+    batch = JKBatch(mols)
+    ref = batch.get_jk(dms)
+    info = batch.info()
+    with tempfile.TemporaryDirectory() as d:
+        for grab, gm in ((1, 1), (2, 2), (64, 1), (1024, 2)):
+            path = os.path.join(d, 'c%d_%d.txt' % (grab, gm))
+            with open(path, 'w') as f:
+                for k in info:
+                    lg = max(0, int(k['tasks']).bit_length() - 1)
+                    f.write('%d %d %d 0 %d %d %d 1.0\n' % (
+                        k['class'], k['np_ij'], k['np_kl'], lg, grab, gm))
+            b = JKBatch(mols, vhfopts=batch.opts)
+            b.tune(dms, cache=path)
+            assert all(k['fp64']['grab'] == grab for k in b.info())
+            got = b.get_jk(dms)
+            for (aj, ak), (bj, bk) in zip(ref, got):
+                assert abs(aj - bj).max() <= 1e-10, (grab, gm)
+                assert abs(ak - bk).max() <= 1e-10, (grab, gm)
+            b.close()
+    batch.close()

@@ -50,7 +50,7 @@ def test_product_tables_match_oracle_tables():
     import oracle
     lib = jklib.load_library()
     rng = np.random.default_rng(0)
-    for n in range(1, 12):
+    for n in range(1, 14):
         for x in np.concatenate([[0., 1e-12, 2., 39.999, 98.0, 150.],
                                  rng.uniform(0, 110, 40)]):
             s = np.zeros(n)
@@ -60,3 +60,32 @@ def test_product_tables_match_oracle_tables():
             so, wo = oracle.rys_roots(n, x)
             np.testing.assert_allclose(s, so, rtol=5e-14, atol=0)
             np.testing.assert_allclose(w, wo, rtol=0, atol=5e-15 * w.sum())
+
+
+def test_shard_plan_balances_and_is_deterministic():
+    """jk_shard_plan (host code): every task gets one owner in range, the
+    plan is the longest-processing-time rule (restated here), identical on
+    repeated calls, and no owner exceeds the mean load by more than the
+    largest task."""
+    lib = jklib.load_library()
+    rng = np.random.default_rng(3)
+    for n, k in ((1, 1), (5, 8), (300, 2), (666, 4), (1000, 8)):
+        cost = np.ascontiguousarray(rng.lognormal(0., 2., n))
+        own = np.zeros(n, dtype=np.int32)
+        assert lib.jk_shard_plan(cost.ctypes.data, n, k, own.ctypes.data) == 0
+        own2 = np.zeros(n, dtype=np.int32)
+        assert lib.jk_shard_plan(cost.ctypes.data, n, k, own2.ctypes.data) == 0
+        np.testing.assert_array_equal(own, own2)
+        assert own.min() >= 0 and own.max() < k
+        ref = np.zeros(n, dtype=np.int32)
+        load = np.zeros(k)
+        for i in sorted(range(n), key=lambda i: (-cost[i], i)):
+            r = int(np.argmin(load))
+            ref[i] = r
+            load[r] += cost[i]
+        np.testing.assert_array_equal(own, ref)
+        loads = np.bincount(own, weights=cost, minlength=k)
+        assert loads.max() <= cost.sum() / k + cost.max() + 1e-9
+    bad = np.zeros(1, dtype=np.int32)
+    assert lib.jk_shard_plan(None, 1, 2, bad.ctypes.data) == 3
+    assert lib.jk_shard_plan(np.ones(1).ctypes.data, 1, 0, bad.ctypes.data) == 3

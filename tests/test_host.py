@@ -170,3 +170,31 @@ def test_bins_and_group_split_match_oracle():
         y = hf_oracle._split_l_ctr_groups(uniq, counts, gs)
         assert np.array_equal(x[0], y[0]) and np.array_equal(x[1], y[1])
         assert x[1].sum() == counts.sum()
+
+
+def test_bench_reference_arm_ranks():
+    """bench.py --impl reference under several ranks: rank 0 alone runs the
+    CPU arm and prints one JSON line; other ranks exit 0 without output.
+    The arm maps no engine library."""
+    import json
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    base = [sys.executable, os.path.join(root, 'bench.py'), '--impl',
+            'reference', '--gpus', '2', '--steps', '1', '--warmup', '0',
+            '--ref-sample-s', '0.3', '--no-reference-gpu', '--workload',
+            'h2o8-dz']
+    env = dict(os.environ, WORLD_SIZE='2')
+    p1 = subprocess.run(base, env=dict(env, RANK='1'), capture_output=True,
+                        text=True, timeout=300)
+    assert p1.returncode == 0 and p1.stdout.strip() == ''
+    p0 = subprocess.run(base, env=dict(env, RANK='0'), capture_output=True,
+                        text=True, timeout=600)
+    assert p0.returncode == 0, p0.stderr[-2000:]
+    lines = [x for x in p0.stdout.splitlines() if x.strip()]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d['impl'] == 'reference' and d['value'] > 0
+    assert d['cpu_baseline']['kind'] == 'port'
+    assert d['e2e']['h2d_bytes_per_step'] == 0

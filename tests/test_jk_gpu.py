@@ -92,7 +92,7 @@ def test_device_rys_tables_match_host():
     xs = np.concatenate([[0., 1e-13, 0.5, 0.7499, 0.75, 1.0, 2.0, 41.9, 42.0,
                           97.9, 200., 1e5], rng.uniform(0, 120, 200)])
     dx = torch.as_tensor(xs, device='cuda')
-    for n in range(1, 12):
+    for n in range(1, 14):
         for mode in range(3):
             ds = torch.zeros(len(xs) * n, dtype=torch.float64, device='cuda')
             dw = torch.zeros_like(ds)
@@ -291,3 +291,108 @@ def test_full_size_workloads_vs_oracle(name):
     print('%s: oracle full build %.1f s' % (name, time.perf_counter() - t))
     _close(vj, rj)
     _close(vk, rk)
+
+
+def _i_shell_mol(nw, seed=2):
+    """Water molecules in the 6-31G* stand-in plus i shells (an uncontracted
+    and a two-primitive i on O, an i on H) and a g on O: classes with an i
+    shell run the generic kernel at its l = 6 sizes (13 Rys roots at
+    (ii|ii)); the reference sends these quartets to PySCF on the CPU
+    (cuobc/scf/hf.py:185-218)."""
+    from byteqc_b200.gto import basis as basis_mod
+    extra = {'O': [[6, [1.3, 1.0]], [6, [2.5, 0.7], [0.6, 0.5]],
+                   [4, [1.0, 1.0]]],
+             'H': [[6, [0.9, 1.0]]]}
+    bas = {s: list(basis_mod.load('standin-6-31g*', s)) + extra[s]
+           for s in ('O', 'H')}
+    return Mole(atom=geom.water_cluster(nw, box=5.0, seed=seed),
+                basis=bas).build()
+
+
+@pytest.mark.parametrize('nw', [1, 2])
+def test_get_jk_i_shells_vs_oracle(nw):
+    from byteqc_b200.cuobc.scf import hf
+    from oracle import hf_oracle
+    mol = _i_shell_mol(nw)
+    assert int(mol._bas[:, 1].max()) == 6
+    opt = hf._VHFOpt(mol).build()
+    ropt = hf_oracle.VHFOpt(mol).build()
+    np.testing.assert_allclose(opt.q_cond, ropt.q_cond, rtol=1e-11,
+                               atol=1e-16)
+    np.testing.assert_array_equal(opt.bas_pairs_locs, ropt.bas_pairs_locs)
+    dm = _rand_dm(mol.nao, ndm=2)
+    rj, rk = hf_oracle.get_jk(mol, dm, vhfopt=ropt)
+    vj, vk = hf.get_jk(mol, dm, vhfopt=opt)
+    _close(vj, rj)
+    _close(vk, rk)
+    cj, ck = hf.get_jk_class_pairs(mol, dm, opt)
+    _close(cj.cpu().numpy(), rj)
+    _close(ck.cpu().numpy(), rk)
+
+
+def test_batch_and_fill_i_shells():
+    """Batched builds with i shells match single builds, and the ERI-tensor
+    fill of classes with an i shell matches the oracle's shell quartets."""
+    from byteqc_b200.cuobc.lib import int4c
+    from byteqc_b200.cuobc.scf import hf
+    from byteqc_b200.cuobc.scf.batch import JKBatch
+    import oracle
+    mols = [_i_shell_mol(1, seed=s) for s in (3, 4)]
+    dms = [_rand_dm(m.nao, seed=5 + i) for i, m in enumerate(mols)]
+    batch = JKBatch(mols)
+    res = batch.get_jk(dms)
+    for m, (mol, dm, opt) in enumerate(zip(mols, dms, batch.opts)):
+        vj, vk = hf.get_jk(mol, dm, vhfopt=opt)
+        _close(res[m][0], vj)
+        _close(res[m][1], vk)
+    batch.close()
+    mol = mols[0]
+    opt = hf._VHFOpt(mol).build(diag_block_with_triu=True)
+    pm = opt.mol
+    ls = opt.uniq_l_ctr[:, 0]
+    ngr = len(ls)
+    ao_loc = pm.ao_loc_nr(cart=True)
+    offs = opt.l_ctr_offsets
+    cp_idx, cp_jdx = np.tril_indices(ngr)
+    tested = 0
+    for cp_ij in range(len(opt.log_qs)):
+        for cp_kl in range(cp_ij + 1):
+            g = (cp_idx[cp_ij], cp_jdx[cp_ij], cp_idx[cp_kl], cp_jdx[cp_kl])
+            if 6 not in [int(ls[x]) for x in g] or tested >= 6:
+                continue
+            si, sj, sk, sl, blk = int4c.get_int4c_slice(cp_ij, cp_kl, opt)
+            blk = blk.cpu().numpy()
+            # every quartet of the first shell of each group (pair lists
+            # keep them: all survive the Schwarz cutoff here)
+            shells = [int(offs[x]) for x in g]
+            ref = oracle.eri_shells(pm, *shells)
+            a0 = [int(ao_loc[s]) - int(ao_loc[offs[x]]) for s, x in zip(shells, g)]
+            n = ref.shape
+            got = blk[a0[0]:a0[0] + n[0], a0[1]:a0[1] + n[1],
+                      a0[2]:a0[2] + n[2], a0[3]:a0[3] + n[3]]
+            assert abs(got - ref).max() <= 1e-10, (g, abs(got - ref).max())
+            tested += 1
+    assert tested > 0
+
+
+def test_sharded_get_jk_two_ranks():
+    """get_jk(..., group=...) split over two ranks (gloo, both on this GPU:
+    their kernels never wait on each other, the all-reduce goes through the
+    host) equals the unsharded build on every rank, FP64, two densities,
+    mixed, J only."""
+    import os
+    import socket
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    with socket.socket() as so:
+        so.bind(('127.0.0.1', 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, '-m', 'torch.distributed.run', '--nnodes=1',
+           '--nproc-per-node=2', '--master-addr=127.0.0.1',
+           '--master-port=%d' % port,
+           os.path.join(root, 'tests', 'shard_worker.py')]
+    p = subprocess.run(cmd, cwd=root, capture_output=True, text=True,
+                       timeout=600)
+    assert p.returncode == 0, (p.stdout + p.stderr)[-3000:]
+    assert 'rank 0 ok' in p.stdout and 'rank 1 ok' in p.stdout

@@ -42,10 +42,10 @@ def test_ss_closed_form():
 
 def test_rys_quadrature_exact_on_moments():
     """sum_r w_r t_r^(2k) = F_k(x) for k < 2n (the Rys rule integrates the
-    Boys moments exactly), n = 1..11 on x in [0, 120]."""
+    Boys moments exactly), n = 1..13 on x in [0, 120]."""
     import oracle
     from oracle.eri_os import boys
-    for n in range(1, 12):
+    for n in range(1, 14):
         for x in (0.0, 0.3, 1.7, 6.0, 25.0, 60.0, 119.0):
             s, w = oracle.rys_roots(n, x)
             for k in range(2 * n):
@@ -277,11 +277,11 @@ def test_basis_conventions_independent_of_product():
     """The oracle's radial normalisation and Cartesian-to-spherical matrix
     (oracle/gto_oracle.py: scipy's gamma function and spherical harmonics)
     against the product's (byteqc_b200.gto.mole: closed-form solid
-    harmonics) for l = 0..5; the two are derived independently, so a wrong
+    harmonics) for l = 0..6; the two are derived independently, so a wrong
     matrix or norm cannot cancel between the engine and the oracle."""
     from byteqc_b200.gto import mole
     from oracle import gto_oracle
-    for l in range(6):
+    for l in range(7):
         np.testing.assert_allclose(gto_oracle.cart2sph(l), mole.cart2sph(l),
                                    rtol=0, atol=5e-14)
         e = np.array([0.07, 0.9, 13.0, 4000.0])
@@ -290,17 +290,26 @@ def test_basis_conventions_independent_of_product():
 
 
 @pytest.mark.parametrize('basis', ['standin-cc-pvdz', 'standin-def2-tzvp',
-                                   'standin-6-31g*'])
+                                   'standin-6-31g*', 'i-shells'])
 def test_contracted_spherical_overlap_is_normalised(basis):
     """Every contracted spherical function has unit norm under the oracle's
     own overlap integrals (Obara-Saika, jk_oracle.c) and transforms, and the
-    overlap matrix equals the product's one-electron code."""
+    overlap matrix equals the product's one-electron code; also for a basis
+    with g, h and i shells."""
     from oracle import gto_oracle
+    if basis == 'i-shells':
+        from byteqc_b200.gto import basis as basis_mod
+        extra = {'O': [[4, [1.1, 1.0]], [5, [0.9, 1.0]],
+                       [6, [2.5, 0.7], [0.6, 0.5]]],
+                 'H': [[6, [0.9, 1.0]]]}
+        basis = {s: list(basis_mod.load('standin-cc-pvdz', s)) + extra[s]
+                 for s in ('O', 'H')}
     mol = Mole(atom=geom.water_cluster(2, box=5.0, seed=0),
                basis=basis).build()
     s = gto_oracle.overlap(mol)
     assert abs(np.diag(s) - 1).max() < 1e-13
-    np.testing.assert_allclose(s, mol.intor('int1e_ovlp'), rtol=0, atol=1e-13)
+    # (i shells: the two recursions round differently at about 1e-13)
+    np.testing.assert_allclose(s, mol.intor('int1e_ovlp'), rtol=0, atol=5e-13)
 
 
 @pytest.mark.parametrize('basis', ['standin-cc-pvdz', 'standin-def2-tzvp',
@@ -354,3 +363,29 @@ def test_pair_data_matches_reference_cache(basis):
         assert got == n
         np.testing.assert_array_equal(mine, ref)
         gint.GINTdel_basis_prod(ctypes.byref(cache))
+
+
+def test_eri_vs_obara_saika_i_shells():
+    """Quartets with i shells (l = 6; the reference hands these to PySCF on
+    the CPU, the engine runs them in its generic GPU kernel with up to 13
+    Rys roots): the oracle's Rys engine against Obara-Saika."""
+    import oracle
+    from oracle import eri_os
+    from oracle import hf_oracle
+    from byteqc_b200.gto import basis as basis_mod
+    extra = {'O': [[6, [1.3, 1.0]], [6, [2.5, 0.7], [0.6, 0.5]]],
+             'H': [[6, [0.9, 1.0]]]}
+    bas = {s: list(basis_mod.load('standin-6-31g*', s)) + extra[s]
+           for s in ('O', 'H')}
+    mol = Mole(atom=geom.water_cluster(1, box=4.0, seed=3), basis=bas).build()
+    pm = hf_oracle.VHFOpt(mol).build().mol
+    rng = np.random.default_rng(1)
+    ls = pm._bas[:, 1]
+    by_l = {l: np.flatnonzero(ls == l) for l in (0, 1, 2, 6)}
+    for lq in [(6, 0, 0, 0), (6, 1, 1, 0), (6, 2, 0, 0), (6, 6, 0, 0),
+               (6, 0, 6, 0)]:
+        sh = [int(rng.choice(by_l[l])) for l in lq]
+        a = oracle.eri_shells(pm, *sh)
+        b = eri_os.eri_shells(pm, *sh)
+        assert a.shape == b.shape
+        assert abs(a - b).max() <= 1e-12 * abs(b).max() + 1e-14, lq

@@ -40,16 +40,52 @@ def test_result_same_alone_and_in_the_mix():
 
 
 def test_admission_by_memory_budget():
+    """Admission bounds each request's footprint from its basis before
+    anything is allocated: with room for two bounds at a time, never more
+    than two requests are active and no basis handle is built for a
+    request that waits."""
     from byteqc_b200.cuobc.scf import hf
-    from byteqc_b200.cuobc.scf.serve import JKServer, footprint_bytes
+    from byteqc_b200.cuobc.scf.serve import JKServer, footprint_bound_bytes
     mols = [_mol(5, 20 + i, 'standin-cc-pvdz') for i in range(4)]
-    need = max(footprint_bytes(hf._VHFOpt(m).build()) for m in mols)
-    srv = JKServer(hbm_budget_bytes=int(2.5 * need), n_iter=3)
+    need = max(footprint_bound_bytes(m) for m in mols)
+    built = []
+    orig = hf._VHFOpt.build
+
+    def counting_build(self, *a, **k):
+        built.append(self)
+        return orig(self, *a, **k)
+    hf._VHFOpt.build = counting_build
+    try:
+        srv = JKServer(hbm_budget_bytes=int(2.5 * need), n_iter=3)
+        for m in mols:
+            srv.submit(m)
+        while srv.waiting or srv.active:
+            srv.step()
+            assert len(srv.active) <= 2
+            assert len(built) == len(srv.active) + len(srv.finished)
+            assert srv.used <= srv.budget
+    finally:
+        hf._VHFOpt.build = orig
+    assert len(srv.finished) == 4
+
+
+def test_scf_to_convergence_and_batch_reuse():
+    """conv_tol ends a request once its energy change is below it; the final
+    energy equals the RHF driver's; the engine batch is rebuilt only when
+    the set of active requests changes."""
+    from byteqc_b200.cuobc.scf import RHF
+    from byteqc_b200.cuobc.scf.serve import JKServer
+    mols = [Mole(atom=geom.water_cluster(n, box=5.0, seed=30 + n),
+                 basis='standin-6-31g*').build() for n in (1, 2)]
+    srv = JKServer(n_iter=60, conv_tol=1e-10)
     for m in mols:
         srv.submit(m)
-    peak = 0
-    while srv.waiting or srv.active:
-        srv.step()
-        peak = max(peak, len(srv.active) + (1 if srv.finished else 0))
-        assert srv.used <= srv.budget
-    assert len(srv.finished) == 4
+    srv.run_until_empty()
+    assert all(r.converged for r in srv.finished)
+    assert srv.batch_builds < srv.steps
+    for r in srv.finished:
+        mf = RHF(r.mol)
+        e = mf.kernel()
+        assert abs(r.energies[-1] - e) < 1e-8, (r.energies[-1], e)
+    st = srv.stats()
+    assert st['iteration_p50_ms'] >= st['build_p50_ms'] * 0.5
