@@ -317,7 +317,7 @@ static int batch_segments(jk_batch* t, const double* const* dms, double* const* 
     }
     std::vector<JKSeg> s64(std::max(1, t->nseg)), s32(std::max(1, t->nseg));
     int i = 0;
-    for (auto& k : t->keys)
+    for (auto& k : t->keys) {
         for (auto& sgi : k.segs) {
             int m = sgi.first;
             jk_internal_fill_seg_batch(t->mols[m], sgi.second, dms[m], n_dm, vjs ? vjs[m] : nullptr,
@@ -342,6 +342,7 @@ static int batch_segments(jk_batch* t, const double* const* dms, double* const* 
             }
             i++;
         }
+    }
     t->h_dmc.resize(t->nmol);
     for (int m = 0; m < t->nmol; m++) {
         jk_basis* b = t->mols[m];
@@ -440,10 +441,11 @@ extern "C" int jk_batch_build(jk_batch_t* t, const double* const* dms, double* c
 // launch shapes are timed on this batch with CUDA events, each launch alone
 // on the caller's stream after the bookkeeping of a real build, and the
 // fastest is kept.  Candidates: static chunks; the persistent mode at one
-// and two resident grids with three grab sizes (tasks per warp for the
-// thread kernels, per team for the team kernels, per block for the generic
-// kernel).  A cache file keeps the choices per (class, primitive counts,
-// part, log2 of the task count); keys found there are not timed again.
+// resident grid with three grab sizes (tasks per warp for the thread
+// kernels, per team for the team kernels, per block for the generic kernel)
+// and at two resident grids with the middle one.  A cache file keeps the
+// choices per (class, primitive counts, part, log2 of the task count); keys
+// found there are not timed again.
 // ---------------------------------------------------------------------------
 static bool class_is_generic(int cls) {
     const int ll = cls % 7, lk = (cls / 7) % 7, lj = (cls / 49) % 7, li = cls / 343;
@@ -507,12 +509,16 @@ extern "C" int jk_batch_tune(jk_batch_t* t, const double* const* dms, double* co
             int g[3];
             cand_grabs(key.cls, g);
             std::vector<JKBatchCfg> cands = {{nullptr, 0, 1}};
-            for (int gm = 1; gm <= 2; gm++)
-                for (int i = 0; i < 3; i++) cands.push_back({nullptr, g[i], gm});
+            for (int i = 0; i < 3; i++) cands.push_back({nullptr, g[i], 1});
+            cands.push_back({nullptr, g[1], 2});
+            // untimed first launch (attributes, instruction cache)
+            BCUDA(cudaMemsetAsync(t->d_queue, 0, sizeof(unsigned long long) * 2 * nkeys, st));
+            rc = batch_launch_key(t, k, part, cands[0], st);
+            if (rc) return rc;
             float best = -1.f;
             for (const JKBatchCfg& c : cands) {
                 float tmin = -1.f;
-                for (int rep = 0; rep < 2; rep++) {
+                for (int rep = 0; rep < 1; rep++) {
                     BCUDA(cudaMemsetAsync(t->d_queue, 0, sizeof(unsigned long long) * 2 * nkeys, st));
                     BCUDA(cudaEventRecord(e0, st));
                     rc = batch_launch_key(t, k, part, c, st);

@@ -107,6 +107,41 @@ __device__ __forceinline__ void boys01(double x, double& f0, double& f1) {
     }
 }
 
+// Rys node r at x with the root count N known at run time (the layout and
+// evaluation of rys_root<N>)
+__device__ __forceinline__ void rys_root_rt(const double* __restrict__ rys, int N, double x, int r, double& s, double& w) {
+    if (N == 1) {
+        double f0, f1;
+        boys01(x, f0, f1);
+        w = f0;
+        s = f1 / f0;
+        return;
+    }
+    if (x >= rys_xmax_c(N)) {
+        const int b = N * (N - 1) / 2 + r;
+        const double rx = 1. / x;
+        s = rys_herm_r[b] * rx;
+        w = rys_herm_w[b] * sqrt(rx);
+        return;
+    }
+    const int m = (int)(x * 0.5);
+    const double t = x - (2 * m + 1), tt = t + t;
+    const double* c = rys + rys_off_c(N) + (size_t)(m * 2 * N) * RYS_NC;
+    const double* cs = c + r * RYS_NC;
+    const double* cw = c + (N + r) * RYS_NC;
+    double b1 = 0., b2 = 0., v1 = 0., v2 = 0.;
+    for (int k = RYS_NC - 1; k >= 1; k--) {
+        double b0 = fma(tt, b1, __ldg(cs + k) - b2);
+        b2 = b1;
+        b1 = b0;
+        b0 = fma(tt, v1, __ldg(cw + k) - v2);
+        v2 = v1;
+        v1 = b0;
+    }
+    s = fma(t, b1, __ldg(cs) - b2);
+    w = fma(t, v1, __ldg(cw) - v2);
+}
+
 // all N roots at x from the shared-memory table
 template <int N>
 __device__ __forceinline__ void rys_roots_all(const double* __restrict__ tab, double x, double* s, double* w) {
@@ -516,14 +551,6 @@ struct JKSeg {
     double* jp_ij;
     double* jp_kl;
     int np_ij, np_kl;        // pairs of each class (component stride)
-    // K through per-warp row buffers (jk_build's single-segment thread
-    // kernels, one density): first AO and AO count of the groups of the ket
-    // pair's two shells, and the buffer size per warp in doubles (0: off).
-    // rb_allowed: the caller accepts either orientation of a K element in
-    // the raw buffer (jk_build; the class-pair entries keep the reference's)
-    int kao0, nk, lao0, nl;
-    int rb_words;
-    int rb_allowed;
     long long pk_stride;     // packed elements per density
     int ls[4];               // angular momenta of the class (read by the generic kernel)
 };

@@ -42,41 +42,6 @@ struct JKGen {
 };
 static_assert(JKGen<5>::SMEM <= 227 * 1024 && JKGen<6>::SMEM <= 227 * 1024, "generic kernel shared memory");
 
-// Rys node r at x with the root count N known at run time (the layout and
-// evaluation of rys_root<N>)
-__device__ void rys_root_rt(const double* __restrict__ rys, int N, double x, int r, double& s, double& w) {
-    if (N == 1) {
-        double f0, f1;
-        boys01(x, f0, f1);
-        w = f0;
-        s = f1 / f0;
-        return;
-    }
-    if (x >= rys_xmax_c(N)) {
-        const int b = N * (N - 1) / 2 + r;
-        const double rx = 1. / x;
-        s = rys_herm_r[b] * rx;
-        w = rys_herm_w[b] * sqrt(rx);
-        return;
-    }
-    const int m = (int)(x * 0.5);
-    const double t = x - (2 * m + 1), tt = t + t;
-    const double* c = rys + rys_off_c(N) + (size_t)(m * 2 * N) * RYS_NC;
-    const double* cs = c + r * RYS_NC;
-    const double* cw = c + (N + r) * RYS_NC;
-    double b1 = 0., b2 = 0., v1 = 0., v2 = 0.;
-    for (int k = RYS_NC - 1; k >= 1; k--) {
-        double b0 = fma(tt, b1, __ldg(cs + k) - b2);
-        b2 = b1;
-        b1 = b0;
-        b0 = fma(tt, v1, __ldg(cw + k) - v2);
-        v2 = v1;
-        v1 = b0;
-    }
-    s = fma(t, b1, __ldg(cs) - b2);
-    w = fma(t, v1, __ldg(cw) - v2);
-}
-
 // One Rys 2D block at run-time angular momenta: the recursion of rys_2d,
 // output I[((i*(lj+1)+j)*(lk+1)+k)*(ll+1)+l].  The intermediate arrays live
 // in the caller's shared-memory scratch W (JKGen<GL>::W doubles), not on the

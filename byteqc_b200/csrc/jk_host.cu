@@ -833,15 +833,6 @@ static void fill_seg(const jk_basis* b, int cp_ij, int cp_kl, const long long* q
     s->jp_ij = s->jp_kl = nullptr;
     s->np_ij = s->np_kl = 0;
     s->pk_stride = 0;
-    {
-        const int gk = b->h_cls_gi[cp_kl], gl = b->h_cls_gj[cp_kl];
-        s->kao0 = b->h_ao_loc[b->h_group_off[gk]];
-        s->nk = b->h_ao_loc[b->h_group_off[gk + 1]] - s->kao0;
-        s->lao0 = b->h_ao_loc[b->h_group_off[gl]];
-        s->nl = b->h_ao_loc[b->h_group_off[gl + 1]] - s->lao0;
-        s->rb_words = 0;
-        s->rb_allowed = 0;
-    }
     s->ls[0] = b->h_group_l[b->h_cls_gi[cp_ij]];
     s->ls[1] = b->h_group_l[b->h_cls_gj[cp_ij]];
     s->ls[2] = b->h_group_l[b->h_cls_gi[cp_kl]];
@@ -926,7 +917,6 @@ extern "C" int jk_build(jk_basis_t* b, const double* dm, int n_dm, double* vj, d
         const JKScreenCQ& cq = b->h_cq[c];
         JKSeg seg;
         fill_seg(b, cq.cp_ij, cq.cp_kl, b->d_qoff + cq.qoff_off, cq.n_ij, dm, n_dm, vj, vk, &seg);
-        seg.rb_allowed = 1;
         if (packed) {
             const JKPackCls &ki = b->h_pack[cq.cp_ij], &kk = b->h_pack[cq.cp_kl];
             seg.dp_ij = dp + ki.off;
@@ -1242,6 +1232,13 @@ __global__ void jk_rys_eval_kernel(const double* rys, const double* x, int count
                 w[i * N + r] = rw;
             }
         }
+    } else if (mode == 5) {  // run-time root count (generic kernels), global table
+        for (int r = 0; r < N; r++) {
+            double rs, rw;
+            rys_root_rt(rys, N, x[i], r, rs, rw);
+            s[i * N + r] = rs;
+            w[i * N + r] = rw;
+        }
     } else if (mode == 0) {
         double rs[N], rw[N];
         rys_roots_all<N>(tab, x[i], rs, rw);
@@ -1268,8 +1265,8 @@ static cudaError_t rys_eval_launch(const double* rys, const double* x, int count
 }
 
 extern "C" int jk_rys_roots_device(int n, const double* x, int count, double* s, double* w, int mode, void* stream) {
-    if (n < 1 || n > 11 || !x || !s || !w || count < 0 || mode < 0 || mode > 4 ||
-        (mode >= 3 && n > JK_F32_ROOTS))
+    if (n < 1 || n > RYS_NMAX || !x || !s || !w || count < 0 || mode < 0 || mode > 5 ||
+        ((mode == 3 || mode == 4) && n > JK_F32_ROOTS))
         return set_err(JK_ERR_ARG, "jk_rys_roots_device: bad args");
     if (count == 0) return JK_OK;
     const double* rys;
@@ -1288,7 +1285,9 @@ extern "C" int jk_rys_roots_device(int n, const double* x, int count, double* s,
         case 8: e = rys_eval_launch<8>(rys, x, count, s, w, mode, st); break;
         case 9: e = rys_eval_launch<9>(rys, x, count, s, w, mode, st); break;
         case 10: e = rys_eval_launch<10>(rys, x, count, s, w, mode, st); break;
-        default: e = rys_eval_launch<11>(rys, x, count, s, w, mode, st); break;
+        case 11: e = rys_eval_launch<11>(rys, x, count, s, w, mode, st); break;
+        case 12: e = rys_eval_launch<12>(rys, x, count, s, w, mode, st); break;
+        default: e = rys_eval_launch<13>(rys, x, count, s, w, mode, st); break;
     }
     CUDA_TRY(e);
     return JK_OK;

@@ -107,7 +107,6 @@ struct JKTaskCursor {
 // prefix segt[0..nseg]; all segments of a launch share the class and the
 // primitive counts.  Cursors walk increasing task indices.
 struct JKOneSeg {
-    static constexpr bool ROWBUF = true;  // may digest K through row buffers
     const JKSeg& sg;
     const long long* task0;
     __device__ __forceinline__ long long total() const { return task0[1]; }
@@ -123,8 +122,6 @@ struct JKOneSeg {
             row = rc.row;
             return src.sg;
         }
-        // one past the last task of the current row
-        __device__ __forceinline__ long long row_end() const { return rc.rend; }
     };
 };
 
@@ -135,7 +132,6 @@ struct JKOneSeg {
 // waiting on other blocks, only an atomic add per chunk.  Otherwise the
 // tasks are split into equal contiguous chunks over the grid.
 struct JKSegTable {
-    static constexpr bool ROWBUF = false;
     const JKSeg* segs;
     const long long* segt;
     int nseg;
@@ -166,7 +162,6 @@ struct JKSegTable {
             row = rc.row;
             return src.segs[s];
         }
-        __device__ __forceinline__ long long row_end() const { return sbeg + rc.rend; }
     };
 };
 
@@ -361,32 +356,9 @@ __device__ __forceinline__ JKSinkGlobal jk_sink_global(const JKSeg& sg) {
     return JKSinkGlobal{sg.vj, sg.vk, sg.nao, (size_t)sg.nao * sg.nao};
 }
 
-// ---------------------------------------------------------------------------
-// K through per-warp row buffers.  While the lanes of a warp work on
-// quartets of one bra pair (ij) -- a warp takes consecutive columns of a
-// row -- every K contribution of those quartets lands in the rows i and j
-// of K, at the columns of the ket shells' two groups; the density elements
-// they need sit in the same rows of D.  The warp stages D(i, .) and D(j, .)
-// over those columns in shared memory when it enters the row, adds the K
-// contributions into shared-memory rows K(i, .) and K(j, .) (shared-memory
-// atomics: lanes may share a ket shell), and flushes them to global memory
-// with coalesced atomics when it leaves the row, instead of one scattered
-// global atomic and one scattered density load per element and quartet.
-// Layout per warp (doubles, W = nk + nl columns: the k group, then the l
-// group): D rows of i (NFI), D rows of j (NFJ), K rows of i, K rows of j.
-// ---------------------------------------------------------------------------
-struct JKRowBuf {
-    double* base;  // the warp's buffer, or null
-    int W;         // columns per row
-    int kc, lc;    // first column of this quartet's k and l shells
-    bool on;       // this lane digests K through the buffer
-};
-
-#define JK_RB_MIN_TASKS 128  // a row is buffered if this many of its tasks remain in the warp's chunk
-
 template <class C, typename R, int NI, class Sink>
 __device__ __forceinline__ void jk_thread_digest(const JKSeg& sg, const JKQuartet& q, int CI0, const R* acc,
-                                                 const Sink& sink, const JKRowBuf& rb) {
+                                                 const Sink& sink) {
     const int nao = sg.nao;
     const int i0 = q.i0 + CI0, j0 = q.j0;
     const int k0 = q.k0, l0 = q.l0;
@@ -472,57 +444,7 @@ __device__ __forceinline__ void jk_thread_digest(const JKSeg& sg, const JKQuarte
                     sink.jkl(idm, k0 + k, l0 + l, v);
                 }
         }
-        if (sg.vk && rb.on && idm == 0) {
-            const int W = rb.W;
-            const double* Di = rb.base;
-            const double* Dj = Di + C::NFI * W;
-            double* Ki = rb.base + (C::NFI + C::NFJ) * W;
-            double* Kj = Ki + C::NFI * W;
-#pragma unroll
-            for (int i = 0; i < NI; i++)
-#pragma unroll
-                for (int k = 0; k < C::NFK; k++) {  // K_ik += (ij|kl) D_jl
-                    double v = 0;
-#pragma unroll
-                    for (int j = 0; j < C::NFJ; j++)
-#pragma unroll
-                        for (int l = 0; l < C::NFL; l++) v += ACC(i, j, k, l) * Dj[j * W + rb.lc + l];
-                    atomicAdd(Ki + (CI0 + i) * W + rb.kc + k, v);
-                }
-#pragma unroll
-            for (int i = 0; i < NI; i++)
-#pragma unroll
-                for (int l = 0; l < C::NFL; l++) {  // K_il += (ij|kl) D_jk
-                    double v = 0;
-#pragma unroll
-                    for (int j = 0; j < C::NFJ; j++)
-#pragma unroll
-                        for (int k = 0; k < C::NFK; k++) v += ACC(i, j, k, l) * Dj[j * W + rb.kc + k];
-                    atomicAdd(Ki + (CI0 + i) * W + rb.lc + l, v);
-                }
-#pragma unroll
-            for (int j = 0; j < C::NFJ; j++)
-#pragma unroll
-                for (int k = 0; k < C::NFK; k++) {  // K_jk += (ij|kl) D_il
-                    double v = 0;
-#pragma unroll
-                    for (int i = 0; i < NI; i++)
-#pragma unroll
-                        for (int l = 0; l < C::NFL; l++) v += ACC(i, j, k, l) * Di[(CI0 + i) * W + rb.lc + l];
-                    atomicAdd(Kj + j * W + rb.kc + k, v);
-                }
-#pragma unroll
-            for (int j = 0; j < C::NFJ; j++)
-#pragma unroll
-                for (int l = 0; l < C::NFL; l++) {  // K_jl += (ij|kl) D_ik
-                    double v = 0;
-#pragma unroll
-                    for (int i = 0; i < NI; i++)
-#pragma unroll
-                        for (int k = 0; k < C::NFK; k++) v += ACC(i, j, k, l) * Di[(CI0 + i) * W + rb.kc + k];
-                    atomicAdd(Kj + j * W + rb.lc + l, v);
-                }
-        } else if (sg.vk) {
+        if (sg.vk) {
 #pragma unroll
             for (int i = 0; i < NI; i++)
 #pragma unroll
@@ -596,8 +518,7 @@ __device__ __forceinline__ void jk_thread_products(R* acc, const R* Ix, const R*
 template <class C, typename R, int CI0, int CI1, class Sink>
 __device__ __forceinline__ void jk_thread_pass(const JKSeg& sg, const JKQuartet& q, const double* __restrict__ tab,
                                                const double* ri, const double* rj, const double* rk,
-                                               const double* rl, const Sink& sink, const JKFillOut* fo,
-                                               const JKRowBuf& rb) {
+                                               const double* rl, const Sink& sink, const JKFillOut* fo) {
     constexpr int NR = C::NROOTS;
     constexpr int NI = CI1 - CI0;
     constexpr int NA = NI * C::NFJ * C::NFK * C::NFL;
@@ -673,64 +594,29 @@ __device__ __forceinline__ void jk_thread_pass(const JKSeg& sg, const JKQuartet&
                                   (double)acc[((i * C::NFJ + j) * C::NFK + k) * C::NFL + l]);
         return;
     }
-    jk_thread_digest<C, R, NI>(sg, q, CI0, acc, sink, rb);
+    jk_thread_digest<C, R, NI>(sg, q, CI0, acc, sink);
 }
 
 
 template <class C, typename R, int PASS, class Sink>
 __device__ __forceinline__ void jk_thread_passes(const JKSeg& sg, const JKQuartet& q, const double* __restrict__ tab,
                                                  const double* ri, const double* rj, const double* rk,
-                                                 const double* rl, const Sink& sink, const JKFillOut* fo,
-                                                 const JKRowBuf& rb) {
+                                                 const double* rl, const Sink& sink, const JKFillOut* fo) {
     constexpr int CI0 = PASS * C::GI;
     if constexpr (CI0 < C::NFI) {
         constexpr int CI1 = CI0 + C::GI < C::NFI ? CI0 + C::GI : C::NFI;
-        jk_thread_pass<C, R, CI0, CI1>(sg, q, tab, ri, rj, rk, rl, sink, fo, rb);
-        jk_thread_passes<C, R, PASS + 1>(sg, q, tab, ri, rj, rk, rl, sink, fo, rb);
+        jk_thread_pass<C, R, CI0, CI1>(sg, q, tab, ri, rj, rk, rl, sink, fo);
+        jk_thread_passes<C, R, PASS + 1>(sg, q, tab, ri, rj, rk, rl, sink, fo);
     }
 }
 
 template <class C, typename R, class Sink>
 __device__ __forceinline__ void jk_thread_quartet(const JKSeg& sg, const JKQuartet& q, const double* __restrict__ tab,
-                                                  const Sink& sink, const JKFillOut* fo = nullptr,
-                                                  const JKRowBuf& rb = JKRowBuf{nullptr, 0, 0, 0, false}) {
+                                                  const Sink& sink, const JKFillOut* fo = nullptr) {
     double ri[3], rj[3], rk[3], rl[3];
     load_pair_centres(sg, q.bij, ri, rj);
     load_pair_centres(sg, q.bkl, rk, rl);
-    jk_thread_passes<C, R, 0>(sg, q, tab, ri, rj, rk, rl, sink, fo, rb);
-}
-
-// stage the D rows of bra shells i0 (NFI rows) and j0 (NFJ rows) over the
-// columns of the ket groups and clear the K rows (first density)
-template <class C>
-__device__ __forceinline__ void jk_rb_stage(const JKSeg& sg, double* base, int i0, int j0, int lane) {
-    const int W = sg.nk + sg.nl, nao = sg.nao;
-    const int nrow = C::NFI + C::NFJ;
-    const double* D = sg.dm;
-    for (int e = lane; e < nrow * W; e += 32) {
-        const int r = e / W, c = e - r * W;
-        const int a = r < C::NFI ? i0 + r : j0 + (r - C::NFI);
-        const int col = c < sg.nk ? sg.kao0 + c : sg.lao0 + (c - sg.nk);
-        base[e] = __ldg(D + col + (size_t)nao * a);
-        base[nrow * W + e] = 0.;
-    }
-}
-
-// add the K rows to vk with coalesced atomics (transposed orientation:
-// consecutive lanes hold consecutive columns; only V + V^T is used)
-template <class C>
-__device__ __forceinline__ void jk_rb_flush(const JKSeg& sg, double* base, int i0, int j0, int lane) {
-    const int W = sg.nk + sg.nl, nao = sg.nao;
-    const int nrow = C::NFI + C::NFJ;
-    const double* K = base + nrow * W;
-    for (int e = lane; e < nrow * W; e += 32) {
-        const double v = K[e];
-        if (v == 0.) continue;
-        const int r = e / W, c = e - r * W;
-        const int a = r < C::NFI ? i0 + r : j0 + (r - C::NFI);
-        const int col = c < sg.nk ? sg.kao0 + c : sg.lao0 + (c - sg.nk);
-        atomicAdd(sg.vk + col + (size_t)nao * a, v);
-    }
+    jk_thread_passes<C, R, 0>(sg, q, tab, ri, rj, rk, rl, sink, fo);
 }
 
 // Resident 128-thread blocks asked of the register allocator (single-segment
@@ -772,11 +658,6 @@ __device__ __forceinline__ void jk_thread_body(const Src& src, double* jk_tab, c
         if (c0 >= total) break;
         long long t = c0 + lane;
         const long long tend = min(total, c0 + chunk);
-        // row buffers (single segment, enabled by the launcher)
-        const JKSeg& sg0 = src.first();
-        const bool rbon = Src::ROWBUF && !fo && sg0.rb_words > 0;
-        double* rbase = jk_tab + RysS<C::NROOTS>::WORDS + (threadIdx.x >> 5) * (rbon ? sg0.rb_words : 0);
-        int rb_bij = -1, rb_skip = -1, rb_i0 = 0, rb_j0 = 0;
         if (t < tend) {
             typename Src::Cursor cur;
             cur.init(src, t);
@@ -785,38 +666,8 @@ __device__ __forceinline__ void jk_thread_body(const Src& src, double* jk_tab, c
                 const JKSeg& sg = cur.seek(src, t, row, col);
                 JKQuartet q = jk_quartet_at(sg, row, col);
                 if (fo) q.norm = JK_FAC;  // the fill has no 1/2 on the ij == kl diagonal
-                JKRowBuf rb{rbase, sg.nk + sg.nl, q.k0 - sg.kao0, sg.nk + q.l0 - sg.lao0, false};
-                if (rbon) {
-                    const unsigned am = __activemask();
-                    if (am == 0xffffffffu) {
-                        const int b0 = __shfl_sync(am, q.bij, 0);
-                        if (b0 != rb_bij && b0 != rb_skip) {
-                            __syncwarp();
-                            if (rb_bij >= 0) jk_rb_flush<C>(sg, rbase, rb_i0, rb_j0, lane);
-                            // tasks of lane 0's row left in this chunk
-                            const long long rem = __shfl_sync(am, min(cur.row_end(), tend) - t, 0);
-                            if (rem >= JK_RB_MIN_TASKS) {
-                                rb_i0 = __shfl_sync(am, q.i0, 0);
-                                rb_j0 = __shfl_sync(am, q.j0, 0);
-                                __syncwarp();
-                                jk_rb_stage<C>(sg, rbase, rb_i0, rb_j0, lane);
-                                rb_bij = b0;
-                                rb_skip = -1;
-                            } else {
-                                rb_bij = -1;
-                                rb_skip = b0;
-                            }
-                            __syncwarp();
-                        }
-                        rb.on = rb_bij >= 0 && q.bij == rb_bij;
-                    }
-                }
-                jk_thread_quartet<C, R>(sg, q, jk_tab, jk_sink_global(sg), fo, rb);
+                jk_thread_quartet<C, R>(sg, q, jk_tab, jk_sink_global(sg), fo);
             }
-        }
-        if (rbon && rb_bij >= 0) {
-            __syncwarp();
-            jk_rb_flush<C>(sg0, rbase, rb_i0, rb_j0, lane);
         }
         if (!queue) break;
     }

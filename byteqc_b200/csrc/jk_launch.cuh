@@ -28,28 +28,13 @@ cudaError_t jk_launch(const JKSeg& seg, const long long* task0, long long max_ta
     using C = JKClass<LI, LJ, LK, LL>;
     if (max_tasks <= 0) return cudaSuccess;
     if constexpr (C::P == 0) {
-        // shared memory per block at the residency the launch bounds ask
-        // for: the Rys table, and the K row buffers of the four warps when
-        // they fit (jk_build's segments, one density)
-        constexpr int minb = JKThreadMinBlocks<C, R>::value;
-        constexpr size_t budget = (size_t)227 * 1024 / minb - 1024;
-        size_t smem = RysS<C::NROOTS>::WORDS * sizeof(double);
-        JKSeg s2 = seg;
-        s2.rb_words = 0;
-        if (seg.rb_allowed && seg.n_dm == 1 && seg.vk) {
-            const long long need = 2LL * (C::NFI + C::NFJ) * (seg.nk + seg.nl);
-            const size_t tot = smem + 4 * (size_t)need * sizeof(double);
-            if (tot <= budget) {
-                s2.rb_words = (int)need;
-                smem = tot;
-            }
-        }
+        constexpr size_t smem = RysS<C::NROOTS>::WORDS * sizeof(double);
         static std::atomic<unsigned long long> attr_done{0};
-        if (cudaError_t e = jk_smem_attr(jk_thread_kernel<C, R>, budget, attr_done); e != cudaSuccess) return e;
+        if (cudaError_t e = jk_smem_attr(jk_thread_kernel<C, R>, smem, attr_done); e != cudaSuccess) return e;
         long long want = (max_tasks + 127) / 128;
         long long cap = (long long)nsm * 16;
         int blocks = (int)(want < cap ? want : cap);
-        jk_thread_kernel<C, R><<<blocks, 128, smem, st>>>(s2, task0);
+        jk_thread_kernel<C, R><<<blocks, 128, smem, st>>>(seg, task0);
     } else {
         using S = JKTeamShape<C>;
         constexpr size_t smem = jk_team_smem<C, R>();

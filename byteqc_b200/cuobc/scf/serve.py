@@ -83,9 +83,11 @@ class _Request:
 
 
 class _SCFState:
-    """Device-resident RHF state of one request (core guess, DIIS)."""
+    """Device-resident RHF state of one request (core guess, DIIS, optional
+    level shift of the virtual space: F + shift (S - S D S / 2), which
+    damps oscillations and leaves the converged energy unchanged)."""
 
-    def __init__(self, req, opt, torch):
+    def __init__(self, req, opt, torch, level_shift=0.):
         mol = req.mol
         dev = dict(dtype=torch.float64, device='cuda')
         self.torch = torch
@@ -102,6 +104,7 @@ class _SCFState:
             _, c = hf.eig(self.h, self.s)
             self.dm = 2. * c[:, :self.nocc] @ c[:, :self.nocc].T
         self.fs, self.es = [], []
+        self.level_shift = level_shift
 
     def update(self, vj, vk):
         torch = self.torch
@@ -124,6 +127,9 @@ class _SCFState:
             rhs[-1] = -1
             coef = torch.linalg.lstsq(b, rhs[:, None]).solution[:n, 0]
             f = sum(ci * fi for ci, fi in zip(coef, self.fs))
+        if self.level_shift:
+            sds = self.s @ self.dm @ self.s
+            f = f + self.level_shift * (self.s - 0.5 * sds)
         _, c = hf.eig(f, self.s)
         self.dm = 2. * c[:, :self.nocc] @ c[:, :self.nocc].T
         return e
@@ -131,7 +137,8 @@ class _SCFState:
 
 class JKServer:
     def __init__(self, hbm_budget_bytes=40 << 30, max_slots=64,
-                 fp32_cutoff=None, n_iter=15, cutoff=1e-13, conv_tol=None):
+                 fp32_cutoff=None, n_iter=15, cutoff=1e-13, conv_tol=None,
+                 level_shift=0.):
         self.torch = hf._torch()
         self.budget = hbm_budget_bytes
         self.max_slots = max_slots
@@ -139,6 +146,7 @@ class JKServer:
         self.n_iter = n_iter
         self.cutoff = cutoff
         self.conv_tol = conv_tol
+        self.level_shift = level_shift
         self.waiting = collections.deque()
         self.active = []  # (request, opt, state, bytes)
         self.finished = []
@@ -169,7 +177,8 @@ class JKServer:
             self.waiting.popleft()
             opt = hf._VHFOpt(req.mol).build(self.cutoff)
             need = footprint_bytes(opt)
-            self.active.append((req, opt, _SCFState(req, opt, self.torch), need))
+            self.active.append((req, opt, _SCFState(req, opt, self.torch,
+                                                    self.level_shift), need))
             self.used += need
 
     def _engine_batch(self):

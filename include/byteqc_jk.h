@@ -182,8 +182,9 @@ int jk_batch_build(jk_batch_t *batch, const double *const *dms, double *const *v
 /* Autotuner of the batch's launch shapes (no reference counterpart: the
  * reference launches a fixed 256-thread shape per class pair and bin,
  * cuobc/lib/gint/gint.h:52).  Times every candidate shape of every class
- * launch of the batch (static chunks; persistent at one or two resident
- * grids with three grab sizes) with CUDA events on `stream`, after the
+ * launch of the batch (static chunks; persistent at one resident grid with
+ * three grab sizes, and at two with the middle one) with CUDA events on
+ * `stream`, after the
  * bookkeeping of a real build with these arguments (same contract as
  * jk_batch_build), and keeps the fastest.  cache_path (may be NULL): a text
  * file of earlier choices per (class, primitive counts, part, log2 task
@@ -213,8 +214,10 @@ int jk_rys_roots_host(int n, double x, double *s, double *w);
  * kernels use (mode 0: all roots from the shared-memory copy, 1: one root at
  * a time from it, 2: one root from the global copy, 3: all roots in single
  * precision as the FP32 quartets of the mixed mode use them, 4: one root at a
- * time in single precision; modes 3 and 4 for n <= 3 only;
- * n = 1 is evaluated from the Boys function in every mode).  x, s, w are device arrays (count,
+ * time in single precision; modes 3 and 4 for n <= 3 only; 5: one root at a
+ * time with the root count known at run time, from the global copy, as the
+ * generic kernels evaluate them; n = 1 is evaluated from the Boys function in
+ * every mode; n <= 13).  x, s, w are device arrays (count,
  * count*n, count*n).  For checking the device evaluation. */
 int jk_rys_roots_device(int n, const double *x, int count, double *s, double *w, int mode, void *stream);
 

@@ -41,9 +41,10 @@ def test_result_same_alone_and_in_the_mix():
 
 def test_admission_by_memory_budget():
     """Admission bounds each request's footprint from its basis before
-    anything is allocated: with room for two bounds at a time, never more
-    than two requests are active and no basis handle is built for a
-    request that waits."""
+    anything is allocated (a request is admitted when the exact footprint of
+    the active ones plus its own bound fits): with room for little more than
+    one bound, one request runs at a time, the device budget is never
+    exceeded, and no basis handle is built for a request that waits."""
     from byteqc_b200.cuobc.scf import hf
     from byteqc_b200.cuobc.scf.serve import JKServer, footprint_bound_bytes
     mols = [_mol(5, 20 + i, 'standin-cc-pvdz') for i in range(4)]
@@ -56,12 +57,12 @@ def test_admission_by_memory_budget():
         return orig(self, *a, **k)
     hf._VHFOpt.build = counting_build
     try:
-        srv = JKServer(hbm_budget_bytes=int(2.5 * need), n_iter=3)
+        srv = JKServer(hbm_budget_bytes=int(1.2 * need), n_iter=3)
         for m in mols:
             srv.submit(m)
         while srv.waiting or srv.active:
             srv.step()
-            assert len(srv.active) <= 2
+            assert len(srv.active) <= 1
             assert len(built) == len(srv.active) + len(srv.finished)
             assert srv.used <= srv.budget
     finally:
