@@ -63,6 +63,11 @@ def make_workload(name, oracle_overlap=False):
     return mol, dm
 
 
+# DRAM bytes (read + write) of one build's class-quartet launches, summed
+# from an ncu launch list of `bench.py --profile-builds 2` on the workload
+PROFILED_TRAFFIC = {'h2o32-tzvp': 78.9e6, 'h2o12-tzvp': 5.7e6}
+
+
 def batch_workload(nmol=256, seed=4, basis='standin-6-31g*'):
     """Seeded molecules of 3-60 atoms grown by a random walk (elements
     C:N:O:H = 3:1:1:5), each with a D = 2 C C^T density.  A molecule with an
@@ -601,9 +606,10 @@ def main():
                     help='molecules of the batched workload (0: skip)')
     ap.add_argument('--batch-steps', type=int, default=1,
                     help='timed repetitions of each batched variant')
-    ap.add_argument('--batch-scf', type=int, default=16,
+    ap.add_argument('--batch-scf', type=int, default=0,
                     help='molecules of the batched workload run to SCF '
-                         'convergence in FP64 and mixed (0: skip)')
+                         'convergence in FP64 and mixed (0: skip; the '
+                         'random-walk geometries converge poorly)')
     ap.add_argument('--batch-scf-iters', type=int, default=50,
                     help='iteration cap of those SCF runs')
     ap.add_argument('--no-rhf', action='store_true',
@@ -612,7 +618,7 @@ def main():
                     help='skip the mixed-precision cutoff sweep with SCF energies')
     ap.add_argument('--sweep-cutoffs', type=float, nargs='*',
                     default=[1e-8, 1e-7, 1e-6, 1e-5, 1e-4])
-    ap.add_argument('--serve-requests', type=int, default=12,
+    ap.add_argument('--serve-requests', type=int, default=8,
                     help='requests of the serving stream (0: skip)')
     ap.add_argument('--serve-iters', type=int, default=15)
     ap.add_argument('--serve-max-nbf', type=int, default=2000,
@@ -794,7 +800,13 @@ def main():
                      'frac': achieved / peak.value if peak.value else None,
                      'peak_source': 'measured FP64 FMA-chain kernel '
                                     '(jk_fma_peak) in this process',
-                     'flops_per_build': flops, 'traffic': None},
+                     'flops_per_build': flops,
+                     'traffic': PROFILED_TRAFFIC.get(args.workload),
+                     'traffic_unit': 'DRAM bytes per build (class launches)',
+                     'traffic_source': 'ncu dram__bytes_read.sum + dram__bytes_write.sum '
+                                       'of `bench.py --profile-builds 2` '
+                                       '(profiles/jk_build_launches_h2o32-tzvp.txt)',
+                     'algorithmic_bytes_per_build': 3 * 8 * int(nao) ** 2},
         'e2e': {'value': world * 1e3 / ms_e2e, 'unit': 'builds/s',
                 'h2d_bytes_per_step': int(dm.nbytes),
                 'd2h_bytes_per_step': int(2 * dm.nbytes)},
