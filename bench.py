@@ -337,10 +337,34 @@ def bench_int4c(args, torch, timed):
     opt = _VHFOpt(mol).build(diag_block_with_triu=True)
     int4c.get_int4c(mol, vhfopt=opt)
     ms = timed(lambda: int4c.get_int4c(mol, vhfopt=opt), 2)
+    # the fill calls alone: every class pair into a preallocated zeroed block
+    from byteqc_b200.cuobc import lib as _lib
+    from byteqc_b200.cuobc.scf.hf import _make_s_index_offsets
+    lib = _lib.load_library()
+    calls = []
+    for cp_ij, cp_kl in zip(*np.tril_indices(len(opt.log_qs))):
+        si, sj, sk, sl, b = int4c.get_int4c_slice(int(cp_ij), int(cp_kl), opt)
+        shp = b.shape
+        calls.append((int(cp_ij), int(cp_kl), b,
+                      np.array([shp[1] * shp[2] * shp[3], shp[2] * shp[3], shp[3], 1], dtype=np.int32),
+                      np.array([si.start, sj.start, sk.start, sl.start], dtype=np.int32),
+                      _make_s_index_offsets(opt.log_qs[cp_ij], 1, opt.direct_scf_tol),
+                      _make_s_index_offsets(opt.log_qs[cp_kl], 1, opt.direct_scf_tol)))
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def fill_calls():
+        for cp_ij, cp_kl, b, st, of, bij, bkl in calls:
+            _lib.check(lib.jk_fill_int2e(
+                opt.handle, ctypes.c_void_p(b.data_ptr()), opt.nao, st.ctypes.data,
+                of.ctypes.data, bij.ctypes.data, bkl.ctypes.data, 1, cp_ij, cp_kl,
+                ctypes.c_void_p(stream)), 'jk_fill_int2e')
+    fill_calls()
+    ms_calls = timed(fill_calls, 3)
     n = opt.nao
     npair = n * (n + 1) // 2
     return {'workload': '(H2O)2 standin-cc-pvdz, working basis',
-            'nao': n, 'ms': ms, 'tensor_gb': 8. * n ** 4 / 1e9,
+            'nao': n, 'ms': ms, 'fill_calls_ms': ms_calls,
+            'class_pairs': len(calls), 'tensor_gb': 8. * n ** 4 / 1e9,
             'unique_integrals_per_s': npair * (npair + 1) // 2 / (ms * 1e-3),
             'tensor_write_gbs': 8. * n ** 4 / (ms * 1e-3) / 1e9}
 
@@ -532,7 +556,33 @@ def run_reference(args):
     }
     if not args.no_reference_gpu:
         line['reference_gpu'] = reference_gpu(args, mol, dm)
+        if not args.no_int4c:
+            line['reference_gpu_int4c'] = reference_gpu_int4c()
     print(json.dumps(line))
+
+
+def reference_gpu_int4c():
+    """The reference's get_int4c flow with its own GINTfill_int2e kernels
+    on this GPU, on the workload of the int4c section ((H2O)2 / cc-pVDZ
+    stand-in, working basis), in a child process; the set-up (groups, pair
+    lists, Schwarz values) is the oracle's restatement of _VHFOpt.build."""
+    from oracle import hf_oracle, ref_jk
+    from byteqc_b200.gto import Mole, geom
+    if not ref_jk.available():
+        return {'unavailable': 'oracle/_ref not built'}
+    mol = Mole(atom=geom.water_cluster(2, box=5.0, seed=0),
+               basis='standin-cc-pvdz').build()
+    ropt = hf_oracle.VHFOpt(mol).build(diag_block_with_triu=True)
+    try:
+        info = ref_jk.run('get_int4c_timing', ropt)
+    except Exception as e:
+        return {'unavailable': str(e)[-300:]}
+    n = info['nao']
+    info.update(workload='(H2O)2 standin-cc-pvdz, working basis',
+                tensor_write_gbs=8. * n ** 4 / (info['ms'] * 1e-3) / 1e9,
+                what='cuobc/lib/int4c.py get_int4c flow over GINTfill_int2e '
+                     '(compiled unmodified for sm_100a)')
+    return info
 
 
 def reference_gpu(args, mol, dm):

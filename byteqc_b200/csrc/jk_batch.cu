@@ -12,6 +12,14 @@
 // segments are ordered by descending task count, so the largest molecules'
 // work is handed out first.
 //
+// Class quartets with at least `solo_tasks` unscreened tasks are not merged:
+// each runs as its own launch of the single-molecule kernel (segment in the
+// parameter bank, as jk_build launches it), in molecule order, fanned out
+// over the side streams ahead of the merged keys.  Such a launch fills the
+// device by itself, and merging it costs more than it saves (measured on
+// 6-31G* molecules of 276-588 functions: 13-36 % slower merged, while
+// molecules below 160 functions build 4.7x faster merged).
+//
 // Launch shape per key (JKBatchCfg): static contiguous chunks, or the
 // persistent mode in which a grid of the device's resident capacity takes
 // chunks from a device counter.  jk_batch_tune times the candidate shapes of
@@ -56,10 +64,19 @@ struct JKBatchKey {
     float tuned_ms[2] = {-1.f, -1.f};
 };
 
+// a class quartet launched on its own (see the top of the file)
+struct JKSolo {
+    int mol, cq, cls;
+    long long tasks;  // unscreened
+    JKSeg s64, s32;   // FP64 and FP32 parts, filled with the segment tables
+};
+
 struct jk_batch {
     int device = 0, nsm = 148, nmol = 0, max_groups = 0;
+    long long solo_tasks = JK_BATCH_SOLO_TASKS;
     std::vector<jk_basis*> mols;
     std::vector<JKBatchKey> keys;
+    std::vector<JKSolo> solo;
     std::vector<int> key_off;  // nkeys + 1 segment offsets
     int nseg = 0;
     JKScreenCQ* d_cq = nullptr;
@@ -172,7 +189,8 @@ static void free_batch(jk_batch* t) {
     delete t;
 }
 
-static int batch_create(jk_basis_t* const* bases, int nmol, jk_batch* t) {
+static int batch_create(jk_basis_t* const* bases, int nmol, long long solo_tasks, jk_batch* t) {
+    t->solo_tasks = solo_tasks;
     BCUDA(cudaGetDevice(&t->device));
     BCUDA(cudaDeviceGetAttribute(&t->nsm, cudaDevAttrMultiProcessorCount, t->device));
     BCUDA(t->fan.init());
@@ -189,6 +207,17 @@ static int batch_create(jk_basis_t* const* bases, int nmol, jk_batch* t) {
             const JKScreenCQ& cq = b->h_cq[c];
             cqs.push_back(cq);
             int cls = jk_internal_class_index(b, cq.cp_ij, cq.cp_kl);
+            const long long n = cq.cp_ij == cq.cp_kl ? (long long)cq.n_ij * (cq.n_ij + 1) / 2
+                                                     : (long long)cq.n_ij * cq.n_kl;
+            if (solo_tasks > 0 && n >= solo_tasks) {
+                JKSolo so{};
+                so.mol = m;
+                so.cq = c;
+                so.cls = cls;
+                so.tasks = n;
+                t->solo.push_back(so);
+                continue;
+            }
             int np_ij = b->h_group_nprim[cq.gi] * b->h_group_nprim[cq.gj];
             int np_kl = b->h_group_nprim[cq.gk] * b->h_group_nprim[cq.gl];
             if (!jk_internal_class_team(cls)) np_ij = np_kl = -1;
@@ -204,8 +233,6 @@ static int batch_create(jk_basis_t* const* bases, int nmol, jk_batch* t) {
                 it = kidx.find(key);
             }
             JKBatchKey& k = t->keys[it->second];
-            const long long n = cq.cp_ij == cq.cp_kl ? (long long)cq.n_ij * (cq.n_ij + 1) / 2
-                                                     : (long long)cq.n_ij * cq.n_kl;
             k.segs.push_back({m, c});
             k.seg_tasks.push_back(n);
             k.max_tasks += n;
@@ -227,6 +254,9 @@ static int batch_create(jk_basis_t* const* bases, int nmol, jk_batch* t) {
     }
     for (auto& k : t->keys)
         if (!jk_internal_batch_launcher(k.cls, 0))
+            return jk_internal_set_err(JK_ERR_UNSUPPORTED, "jk_batch_create: class without kernel");
+    for (auto& so : t->solo)
+        if (!jk_internal_batch_launcher(so.cls, 0))
             return jk_internal_set_err(JK_ERR_UNSUPPORTED, "jk_batch_create: class without kernel");
     t->ncq = (int)cqs.size();
     t->key_off.push_back(0);
@@ -260,10 +290,10 @@ static int batch_create(jk_basis_t* const* bases, int nmol, jk_batch* t) {
     return JK_OK;
 }
 
-extern "C" int jk_batch_create(jk_basis_t* const* bases, int nmol, jk_batch_t** out) {
+extern "C" int jk_batch_create_ex(jk_basis_t* const* bases, int nmol, long long solo_tasks, jk_batch_t** out) {
     if (!bases || nmol <= 0 || !out) return jk_internal_set_err(JK_ERR_ARG, "jk_batch_create: invalid arguments");
     jk_batch* t = new jk_batch();
-    int rc = batch_create(bases, nmol, t);
+    int rc = batch_create(bases, nmol, solo_tasks, t);
     if (rc) {
         free_batch(t);
         *out = nullptr;
@@ -271,6 +301,10 @@ extern "C" int jk_batch_create(jk_basis_t* const* bases, int nmol, jk_batch_t** 
     }
     *out = t;
     return JK_OK;
+}
+
+extern "C" int jk_batch_create(jk_basis_t* const* bases, int nmol, jk_batch_t** out) {
+    return jk_batch_create_ex(bases, nmol, JK_BATCH_SOLO_TASKS, out);
 }
 
 extern "C" int jk_batch_destroy(jk_batch_t* t) {
@@ -315,6 +349,32 @@ static int batch_segments(jk_batch* t, const double* const* dms, double* const* 
         if (!t->d_pmol) BCUDA(cudaMalloc(&t->d_pmol, sizeof(JKPackMol) * t->nmol));
         BCUDA(cudaMemcpy(t->d_pmol, pm.data(), sizeof(JKPackMol) * t->nmol, cudaMemcpyHostToDevice));
     }
+    // pair-packed J side of molecule m's class quartet c in both parts
+    auto set_packed = [&](int m, int c, JKSeg* a, JKSeg* b2) {
+        if (!t->packed) return;
+        const jk_basis* b = t->mols[m];
+        const JKScreenCQ& cq = b->h_cq[c];
+        const JKPackCls &ki = b->h_pack[cq.cp_ij], &kk = b->h_pack[cq.cp_kl];
+        double* dp = t->d_pk + dp_off[m];
+        double* jp = t->d_pk + t->pk_jp + dp_off[m];
+        for (JKSeg* sg : {a, b2}) {
+            sg->dp_ij = dp + ki.off;
+            sg->dp_kl = dp + kk.off;
+            sg->jp_ij = jp + ki.off;
+            sg->jp_kl = jp + kk.off;
+            sg->np_ij = ki.np;
+            sg->np_kl = kk.np;
+            sg->pk_stride = b->pack_total;
+        }
+    };
+    for (auto& so : t->solo) {
+        const int m = so.mol;
+        jk_internal_fill_seg_batch(t->mols[m], so.cq, dms[m], n_dm, vjs ? vjs[m] : nullptr, vks ? vks[m] : nullptr, 0,
+                                   &so.s64);
+        jk_internal_fill_seg_batch(t->mols[m], so.cq, dms[m], n_dm, vjs ? vjs[m] : nullptr, vks ? vks[m] : nullptr, 1,
+                                   &so.s32);
+        set_packed(m, so.cq, &so.s64, &so.s32);
+    }
     std::vector<JKSeg> s64(std::max(1, t->nseg)), s32(std::max(1, t->nseg));
     int i = 0;
     for (auto& k : t->keys) {
@@ -324,22 +384,7 @@ static int batch_segments(jk_batch* t, const double* const* dms, double* const* 
                                        vks ? vks[m] : nullptr, 0, &s64[i]);
             jk_internal_fill_seg_batch(t->mols[m], sgi.second, dms[m], n_dm, vjs ? vjs[m] : nullptr,
                                        vks ? vks[m] : nullptr, 1, &s32[i]);
-            if (t->packed) {
-                const jk_basis* b = t->mols[m];
-                const JKScreenCQ& cq = b->h_cq[sgi.second];
-                const JKPackCls &ki = b->h_pack[cq.cp_ij], &kk = b->h_pack[cq.cp_kl];
-                double* dp = t->d_pk + dp_off[m];
-                double* jp = t->d_pk + t->pk_jp + dp_off[m];
-                for (JKSeg* sg : {&s64[i], &s32[i]}) {
-                    sg->dp_ij = dp + ki.off;
-                    sg->dp_kl = dp + kk.off;
-                    sg->jp_ij = jp + ki.off;
-                    sg->jp_kl = jp + kk.off;
-                    sg->np_ij = ki.np;
-                    sg->np_kl = kk.np;
-                    sg->pk_stride = b->pack_total;
-                }
-            }
+            set_packed(m, sgi.second, &s64[i], &s32[i]);
             i++;
         }
     }
@@ -379,9 +424,11 @@ static int batch_prepare(jk_batch* t, const double* const* dms, double* const* v
     rc = jk_internal_screen(t->d_cq, t->ncq, tol, nbins, prescreen, fp32_cutoff, st);
     if (rc) return rc;
     int nkeys = (int)t->keys.size();
-    jk_seg_prefix_kernel<<<nkeys, 32, 0, st>>>(t->d_cnt64, t->d_key_off, t->d_segt64);
-    BCUDA(cudaGetLastError());
-    if (fp32_cutoff > 0) {
+    if (nkeys > 0) {
+        jk_seg_prefix_kernel<<<nkeys, 32, 0, st>>>(t->d_cnt64, t->d_key_off, t->d_segt64);
+        BCUDA(cudaGetLastError());
+    }
+    if (fp32_cutoff > 0 && nkeys > 0) {
         jk_seg_prefix_kernel<<<nkeys, 32, 0, st>>>(t->d_cnt32, t->d_key_off, t->d_segt32);
         BCUDA(cudaGetLastError());
     }
@@ -420,11 +467,22 @@ extern "C" int jk_batch_build(jk_batch_t* t, const double* const* dms, double* c
     // work counters of the persistent launches start at zero every build
     BCUDA(cudaMemsetAsync(t->d_queue, 0, sizeof(unsigned long long) * 2 * nkeys, st));
     BCUDA(t->fan.begin(st));
-    for (int k = 0; k < nkeys; k++) {
-        rc = batch_launch_key(t, k, 0, t->keys[k].cfg[0], t->fan.pick(2 * k));
+    int lane = 0;  // FP64 parts on the even side streams, FP32 parts on the odd ones
+    for (const JKSolo& so : t->solo) {
+        const JKScreenCQ& cq = t->mols[so.mol]->h_cq[so.cq];
+        rc = jk_internal_launch_part(so.cls, 0, so.s64, cq.task0, so.tasks, t->nsm, t->fan.pick(2 * lane));
         if (rc) return rc;
         if (mixed) {
-            rc = batch_launch_key(t, k, 1, t->keys[k].cfg[1], t->fan.pick(2 * k + 1));
+            rc = jk_internal_launch_part(so.cls, 1, so.s32, cq.task032, so.tasks, t->nsm, t->fan.pick(2 * lane + 1));
+            if (rc) return rc;
+        }
+        lane++;
+    }
+    for (int k = 0; k < nkeys; k++, lane++) {
+        rc = batch_launch_key(t, k, 0, t->keys[k].cfg[0], t->fan.pick(2 * lane));
+        if (rc) return rc;
+        if (mixed) {
+            rc = batch_launch_key(t, k, 1, t->keys[k].cfg[1], t->fan.pick(2 * lane + 1));
             if (rc) return rc;
         }
     }
@@ -556,6 +614,12 @@ extern "C" int jk_batch_tune(jk_batch_t* t, const double* const* dms, double* co
                     kv.second.second);
         fclose(f);
     }
+    return JK_OK;
+}
+
+extern "C" int jk_batch_nsolo(const jk_batch_t* t, int* nsolo) {
+    if (!t || !nsolo) return jk_internal_set_err(JK_ERR_ARG, "jk_batch_nsolo: invalid arguments");
+    *nsolo = (int)t->solo.size();
     return JK_OK;
 }
 

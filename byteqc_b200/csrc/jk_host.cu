@@ -1320,6 +1320,15 @@ int jk_internal_launch(const jk_basis_t* b, int cp_ij, int cp_kl, const JKSeg& s
     return JK_OK;
 }
 
+int jk_internal_launch_part(int class_idx, int fp32, const JKSeg& seg, const long long* d_task0, long long max_tasks,
+                            int nsm, void* stream) {
+    init_tables();
+    jk_launch_fn fn = fp32 ? g_tab32[class_idx] : g_tab64[class_idx];
+    if (!fn) return set_err(JK_ERR_UNSUPPORTED, "no kernel for class %d", class_idx);
+    CUDA_TRY(fn(seg, d_task0, max_tasks, nsm, (cudaStream_t)stream));
+    return JK_OK;
+}
+
 int jk_internal_class_index(const jk_basis_t* b, int cp_ij, int cp_kl) { return class_index(b, cp_ij, cp_kl); }
 
 jk_launch_batch_fn jk_internal_batch_launcher(int class_idx, int fp32) {

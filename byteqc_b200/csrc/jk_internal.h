@@ -155,6 +155,9 @@ struct jk_basis {
 
 // launch one class quartet of basis b as a single segment
 int jk_internal_class_index(const jk_basis_t* b, int cp_ij, int cp_kl);
+// the single-segment launch of a class (FP64 part or FP32 part), as jk_build makes it
+int jk_internal_launch_part(int class_idx, int fp32, const JKSeg& seg, const long long* d_task0, long long max_tasks,
+                            int nsm, void* stream);
 jk_launch_batch_fn jk_internal_batch_launcher(int class_idx, int fp32);
 // 1 if the class runs a team kernel (one primitive count per launch)
 int jk_internal_class_team(int class_idx);

@@ -2,7 +2,9 @@
 
 ``JKBatch(mols)`` builds a _VHFOpt per molecule and one engine batch; then
 ``get_jk(dms)`` returns [(vj, vk), ...] for all molecules from a single
-sequence of launches (one per class shared by the molecules), and
+sequence of launches (one per class shared by the molecules; a class
+quartet of at least ``solo_tasks`` unscreened tasks keeps a launch of its
+own), and
 ``capture(dms)`` / ``replay()`` record that sequence in a CUDA graph so an SCF
 iteration of the whole batch is one graph launch.  ``tune(dms)`` runs the
 engine's autotuner (``jk_batch_tune``): every class launch of the batch is
@@ -27,7 +29,7 @@ def _ptrs(seq):
 
 
 class JKBatch:
-    def __init__(self, mols, cutoff=1e-13, vhfopts=None):
+    def __init__(self, mols, cutoff=1e-13, vhfopts=None, solo_tasks=None):
         torch = hf._torch()
         self.lib = _lib.load_library()
         self.mols = list(mols)
@@ -35,9 +37,19 @@ class JKBatch:
         self.nmol = len(self.mols)
         handles = _ptrs([o.handle.value for o in self.opts])
         self.handle = ctypes.c_void_p()
-        _lib.check(self.lib.jk_batch_create(handles, self.nmol,
-                                            ctypes.byref(self.handle)),
-                   'jk_batch_create')
+        if solo_tasks is None:
+            _lib.check(self.lib.jk_batch_create(handles, self.nmol,
+                                                ctypes.byref(self.handle)),
+                       'jk_batch_create')
+        else:
+            _lib.check(self.lib.jk_batch_create_ex(handles, self.nmol,
+                                                   int(solo_tasks),
+                                                   ctypes.byref(self.handle)),
+                       'jk_batch_create_ex')
+        n = ctypes.c_int()
+        _lib.check(self.lib.jk_batch_nsolo(self.handle, ctypes.byref(n)),
+                   'jk_batch_nsolo')
+        self.nsolo = n.value
         self.nao0 = [o.coeff.shape[1] for o in self.opts]
         self._coeffs = _ptrs([o.coeff_dev.data_ptr() for o in self.opts])
         self._nao0 = (ctypes.c_int * self.nmol)(*self.nao0)

@@ -166,10 +166,18 @@ int jk_get_jk(jk_basis_t *basis, const double *coeff, int nao0, const double *dm
  * molecules' work first, with the same screening decisions as jk_build for
  * each molecule.  Each launch takes static chunks or runs persistent (a grid
  * of the device's resident capacity taking chunks from a device counter),
- * as jk_batch_tune chose; untuned batches use static chunks.
+ * as jk_batch_tune chose; untuned batches use static chunks.  A class
+ * quartet with at least `solo_tasks` unscreened tasks (shell-pair rows x
+ * columns) is not merged: it runs as its own single-molecule launch, as
+ * jk_build makes it; solo_tasks <= 0 merges everything.  jk_batch_create
+ * uses JK_BATCH_SOLO_TASKS.
  */
+#define JK_BATCH_SOLO_TASKS (1LL << 14)
 int jk_batch_create(jk_basis_t *const *bases, int nmol, jk_batch_t **out);
+int jk_batch_create_ex(jk_basis_t *const *bases, int nmol, long long solo_tasks, jk_batch_t **out);
 int jk_batch_destroy(jk_batch_t *batch);
+/* number of class quartets of the batch launched on their own */
+int jk_batch_nsolo(const jk_batch_t *batch, int *nsolo);
 
 /* Per molecule m: dms[m] device density in the working basis, vjs[m]/vks[m]
  * device buffers accumulated as in jk_build (either array may be NULL).  The

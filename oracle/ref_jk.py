@@ -300,6 +300,87 @@ def fill_blocks(vhfopt, pairs, nbins=1, cutoff=None):
         rb.close()
 
 
+def get_int4c_timing(vhfopt, nbins=1, reps=3):
+    """CUDA-event time of the reference's ``get_int4c`` flow
+    (``cuobc/lib/int4c.py:44-70``) on one GPU: for every class pair a zeroed
+    block, ``GINTfill_int2e`` into it, then the eight permuted copies into
+    the dense (nao, nao, nao, nao) tensor; one untimed pass first.  Returns
+    {'ms': mean ms of the whole tensor, 'ms_fill_calls': the fill calls
+    alone (blocks allocated and zeroed beforehand), 'pairs': class pairs}."""
+    import torch
+    from oracle import hf_oracle
+    gint, _ = libs()
+    rb = RefBasis(vhfopt)
+    cutoff = vhfopt.direct_scf_tol
+    ao_loc = vhfopt.mol.ao_loc_nr(cart=True)
+    offs = vhfopt.l_ctr_offsets
+    ncp = len(offs) - 1
+    cp_idx, cp_jdx = np.tril_indices(ncp)
+    npair = len(vhfopt.log_qs)
+    pairs = list(zip(*np.tril_indices(npair)))
+    nao = int(ao_loc[offs[-1]])
+    stream = torch.cuda.current_stream().cuda_stream
+    setup = []
+    for cp_ij, cp_kl in pairs:
+        g = (cp_idx[cp_ij], cp_jdx[cp_ij], cp_idx[cp_kl], cp_jdx[cp_kl])
+        a0 = [int(ao_loc[offs[x]]) for x in g]
+        n = [int(ao_loc[offs[x + 1]]) - a for x, a in zip(g, a0)]
+        st = np.array([n[1] * n[2] * n[3], n[2] * n[3], n[3], 1], dtype=np.int32)
+        of = np.array(a0, dtype=np.int32)
+        bij = hf_oracle.make_s_index_offsets(vhfopt.log_qs[cp_ij], nbins, cutoff)
+        bkl = hf_oracle.make_s_index_offsets(vhfopt.log_qs[cp_kl], nbins, cutoff)
+        sl = [slice(a, a + m) for a, m in zip(a0, n)]
+        setup.append((int(cp_ij), int(cp_kl), n, st, of, bij, bkl, sl))
+
+    def fill(blk, cp_ij, cp_kl, st, of, bij, bkl):
+        err = gint.GINTfill_int2e(rb.gpu, blk.data_ptr(), nao, _ptr(st),
+                                  _ptr(of), _ptr(bij), _ptr(bkl), nbins,
+                                  cp_ij, cp_kl, stream)
+        if err:
+            raise RuntimeError('GINTfill_int2e(%d, %d) returned %d'
+                               % (cp_ij, cp_kl, err))
+
+    def whole():
+        out = torch.zeros((nao,) * 4, dtype=torch.float64, device='cuda')
+        for cp_ij, cp_kl, n, st, of, bij, bkl, (si, sj, sk, sl) in setup:
+            b = torch.zeros(n, dtype=torch.float64, device='cuda')
+            fill(b, cp_ij, cp_kl, st, of, bij, bkl)
+            out[si, sj, sk, sl] = b
+            out[sj, si, sk, sl] = b.permute(1, 0, 2, 3)
+            out[si, sj, sl, sk] = b.permute(0, 1, 3, 2)
+            out[sj, si, sl, sk] = b.permute(1, 0, 3, 2)
+            out[sk, sl, si, sj] = b.permute(2, 3, 0, 1)
+            out[sk, sl, sj, si] = b.permute(2, 3, 1, 0)
+            out[sl, sk, si, sj] = b.permute(3, 2, 0, 1)
+            out[sl, sk, sj, si] = b.permute(3, 2, 1, 0)
+        return out
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    try:
+        ms = timed(whole)
+        blks = [torch.zeros(x[2], dtype=torch.float64, device='cuda') for x in setup]
+
+        def calls():
+            for b, (cp_ij, cp_kl, n, st, of, bij, bkl, _) in zip(blks, setup):
+                fill(b, cp_ij, cp_kl, st, of, bij, bkl)
+        ms_calls = timed(calls)
+        return {'ms': ms, 'ms_fill_calls': ms_calls, 'pairs': len(pairs),
+                'nao': nao}
+    finally:
+        rb.close()
+
+
 def run(func, *args, timeout=1800, **kwargs):
     """Call ``func`` (a name in this module) in a child process."""
     import tempfile

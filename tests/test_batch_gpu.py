@@ -194,3 +194,37 @@ def test_batch_persistent_shapes_match_static():
                 assert abs(ak - bk).max() <= 1e-10, (grab, gm)
             b.close()
     batch.close()
+
+
+def test_batch_solo_class_quartets():
+    """Class quartets above the solo threshold run as their own launches
+    (the single-molecule kernels), the rest merged: every split gives the
+    single-molecule result, in FP64, in mixed precision and from a graph."""
+    from byteqc_b200.cuobc.scf import hf
+    from byteqc_b200.cuobc.scf.batch import JKBatch
+    mols = _mols()
+    dms = _dms(mols, seed=20)
+    base = JKBatch(mols, solo_tasks=0)
+    assert base.nsolo == 0
+    ref = [hf.get_jk(m, d, vhfopt=o) for m, d, o in zip(mols, dms, base.opts)]
+    ref32 = [hf.get_jk(m, d, vhfopt=o, fp32_cutoff=1e-6)
+             for m, d, o in zip(mols, dms, base.opts)]
+    nsolos = []
+    for solo in (1, 64, 4096):
+        b = JKBatch(mols, vhfopts=base.opts, solo_tasks=solo)
+        nsolos.append(b.nsolo)
+        if solo == 1:
+            assert b.info() == []      # everything on its own
+        for cut, want, tol in ((None, ref, 1e-10), (1e-6, ref32, 1e-9)):
+            got = b.get_jk(dms, fp32_cutoff=cut)
+            for (aj, ak), (bj, bk) in zip(want, got):
+                assert abs(aj - bj).max() <= tol, (solo, cut)
+                assert abs(ak - bk).max() <= tol, (solo, cut)
+        b.capture(dms, fp32_cutoff=1e-6)
+        got = b.replay(dms)
+        for (aj, ak), (bj, bk) in zip(ref32, got):
+            assert abs(aj - bj).max() <= 1e-9
+            assert abs(ak - bk).max() <= 1e-9
+        b.close()
+    assert nsolos[0] >= nsolos[1] >= nsolos[2] and nsolos[0] > nsolos[2]
+    base.close()
