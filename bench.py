@@ -284,12 +284,13 @@ def serve_workload(nreq, seed=5, max_nbf=2000, min_nbf=50):
 
 def bench_serve(args, torch):
     """Continuous-batching server on a Poisson stream: the capacity is
-    estimated from one FP64 build of every request alone (sequential, so a
-    lower bound of the batched capacity), then requests arrive at 80 % of
-    that rate, in FP64 and in mixed precision; per-build and per-iteration
-    p50/p99 latency, per-request latency and builds/s."""
-    from byteqc_b200.cuobc.scf import hf
-    from byteqc_b200.cuobc.scf.serve import JKServer, poisson_serve
+    estimated from one FP64 build of every request alone at its starting
+    (core-guess) density (sequential, so a lower bound of the batched
+    capacity), then requests arrive at 80 % of that rate, in FP64 and in
+    mixed precision; per-build and per-iteration p50/p99 latency,
+    per-request latency and builds/s."""
+    from byteqc_b200.cuobc.scf.serve import (JKServer, poisson_serve,
+                                             single_build_seconds)
     mols = serve_workload(args.serve_requests, max_nbf=args.serve_max_nbf)
     nbf = [m.nao for m in mols]
     kw = dict(n_iter=args.serve_iters)
@@ -298,17 +299,7 @@ def bench_serve(args, torch):
     for m in mols[:2]:
         warm.submit(m)
     warm.run_until_empty()
-    build_s = 0.
-    for m in mols:
-        opt = hf._VHFOpt(m).build()
-        dm = np.eye(m.nao) * 0.1
-        hf.get_jk(m, dm, vhfopt=opt, out='device')
-        torch.cuda.synchronize()
-        t = time.perf_counter()
-        hf.get_jk(m, dm, vhfopt=opt, out='device')
-        torch.cuda.synchronize()
-        build_s += time.perf_counter() - t
-        opt.clear()
+    build_s = sum(single_build_seconds(m) for m in mols)
     cap_builds = len(mols) / build_s
     rate = 0.8 * cap_builds / args.serve_iters  # requests per second
     out = {'requests': len(mols), 'iters_per_request': args.serve_iters,

@@ -418,7 +418,6 @@ static void free_basis(jk_basis* b) {
     cudaFree(b->d_pao);
     b->fan.destroy();
     cudaFree(b->d_pk);
-    if (b->h_qoff1) cudaFreeHost(b->h_qoff1);
     if (b->blas) cublasDestroy(b->blas);
     delete b;
 }
@@ -727,6 +726,14 @@ static int create_impl(const int* atm, int natm, const int* bas, int nbas, const
     }
     CUDA_TRY(upload(&b->d_cq, b->h_cq.data(), b->h_cq.size()));
     CUDA_TRY(cudaMalloc(&b->d_task01, sizeof(long long) * 2));
+    // row prefixes of the per-class-pair entries: sized once for the largest
+    // class, so those calls never free a buffer a queued kernel still reads
+    {
+        int mx = 1;
+        for (int c = 0; c < b->ncp; c++) mx = std::max(mx, b->h_pair_locs[c + 1] - b->h_pair_locs[c]);
+        CUDA_TRY(cudaMalloc(&b->d_qoff1, sizeof(long long) * (mx + 1)));
+        b->qoff1_cap = mx + 1;
+    }
     // pair-packed layout of the J side (jk_build)
     b->h_pack.clear();
     b->pack_total = 0;
@@ -950,6 +957,72 @@ extern "C" int jk_build(jk_basis_t* b, const double* dm, int n_dm, double* vj, d
     return JK_OK;
 }
 
+// Row prefix of one class pair's task list from the host bins of the
+// per-class-pair entries (nr_jk_driver.cu:252-280, nr_fill_ao_ints.cu:519-545):
+// row ij in bin s (ij[s] <= ij < ij[s+1]) keeps c_s = kl[nbins - s] - kl[0]
+// columns (none when kl[0] != 0: the reference's bins start at 0), at most
+// ij + 1 of them on a diagonal class pair of jk_build_class_pair; rows below
+// ij[0] or from ij[nbins] on keep none.  The bins go to the device by value,
+// so the entries neither copy nor synchronise.
+#define JK_ROWBINS_MAX 64
+struct JKRowBins {
+    int nbins, diag;
+    int ij[JK_ROWBINS_MAX + 1], kl[JK_ROWBINS_MAX + 1];
+};
+
+// tasks of rows [0, r)
+__host__ __device__ inline long long jk_rowbins_tasks(const JKRowBins& b, long long r) {
+    if (b.kl[0] != 0) return 0;
+    long long acc = 0;
+    for (int s = 0; s < b.nbins; s++) {
+        const long long lo = b.ij[s];
+        const long long hi = r < b.ij[s + 1] ? r : b.ij[s + 1];
+        if (hi <= lo) continue;
+        const long long c = b.kl[b.nbins - s] - b.kl[0];
+        if (!b.diag) {
+            acc += c * (hi - lo);
+        } else {
+            // rows below c keep row + 1 columns, the others c
+            const long long m = lo > (c < hi ? c : hi) ? lo : (c < hi ? c : hi);
+            acc += (m * (m + 1) - lo * (lo + 1)) / 2 + c * (hi - m);
+        }
+    }
+    return acc;
+}
+
+__global__ void jk_rowbins_kernel(const JKRowBins rb, int n_ij, long long* __restrict__ qoff,
+                                  long long* __restrict__ task0) {
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r <= n_ij;
+         r += (long long)gridDim.x * blockDim.x)
+        qoff[r] = jk_rowbins_tasks(rb, r);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        task0[0] = 0;
+        task0[1] = jk_rowbins_tasks(rb, n_ij);
+    }
+}
+
+// bins of a per-class-pair call -> the basis's row prefix and task count, on
+// `st`; returns the task count through *tot
+static int class_pair_rows(jk_basis* b, const int* bins_ij, const int* bins_kl, int nbins, int n_ij, int diag,
+                           cudaStream_t st, long long* tot) {
+    if (nbins > JK_ROWBINS_MAX) return set_err(JK_ERR_ARG, "nbins %d above %d", nbins, JK_ROWBINS_MAX);
+    JKRowBins rb;
+    rb.nbins = nbins;
+    rb.diag = diag;
+    for (int s = 0; s <= nbins; s++) {
+        rb.ij[s] = bins_ij[s];
+        rb.kl[s] = bins_kl[s];
+        if (s && (bins_ij[s] < bins_ij[s - 1] || bins_kl[s] < bins_kl[s - 1]))
+            return set_err(JK_ERR_ARG, "bins must not decrease");
+    }
+    if (n_ij + 1 > (int)b->qoff1_cap) return set_err(JK_ERR_ARG, "class pair larger than the basis' classes");
+    *tot = jk_rowbins_tasks(rb, n_ij);
+    const int blocks = (int)std::min<long long>((n_ij + 256) / 256, (long long)b->nsm * 4);
+    jk_rowbins_kernel<<<blocks, 256, 0, st>>>(rb, n_ij, b->d_qoff1, b->d_task01);
+    CUDA_TRY(cudaGetLastError());
+    return JK_OK;
+}
+
 extern "C" int jk_build_class_pair(jk_basis_t* b, double* vj, double* vk, const double* dm, int nao, int n_dm,
                                    const int* bins_locs_ij, const int* bins_locs_kl, int nbins, int cp_ij,
                                    int cp_kl, void* stream) {
@@ -961,41 +1034,14 @@ extern "C" int jk_build_class_pair(jk_basis_t* b, double* vj, double* vk, const 
     int n_ij = b->h_pair_locs[cp_ij + 1] - b->h_pair_locs[cp_ij];
     // kl bin kb pairs with ij in [bins_ij[0], bins_ij[nbins - kb]) (nr_jk_driver.cu:252-280):
     // row ij (in bin sij) keeps kl < bins_kl[nbins - sij]; diagonal classes keep kl <= ij
-    if ((size_t)n_ij + 1 > b->h_qoff1_cap) {
-        if (b->h_qoff1) cudaFreeHost(b->h_qoff1);
-        CUDA_TRY(cudaMallocHost(&b->h_qoff1, sizeof(long long) * (n_ij + 1)));
-        b->h_qoff1_cap = n_ij + 1;
-    }
-    CUDA_TRY(cudaStreamSynchronize(st));
-    long long* qo = b->h_qoff1;
-    qo[0] = 0;
-    int sij = 0;
-    long long tot = 0;
-    for (int ij = 0; ij < n_ij; ij++) {
-        while (sij < nbins && ij >= bins_locs_ij[sij + 1]) sij++;
-        long long cnt = 0;
-        if (ij >= bins_locs_ij[0] && sij < nbins) {
-            cnt = bins_locs_kl[nbins - sij] - bins_locs_kl[0];
-            if (bins_locs_kl[0] != 0) cnt = 0;  // the reference's bins always start at 0
-            if (cp_ij == cp_kl && cnt > ij + 1) cnt = ij + 1;
-        }
-        tot += cnt;
-        qo[ij + 1] = tot;
-    }
-    if (n_ij + 1 > b->qoff1_cap) {
-        cudaFree(b->d_qoff1);
-        CUDA_TRY(cudaMalloc(&b->d_qoff1, sizeof(long long) * (n_ij + 1)));
-        b->qoff1_cap = n_ij + 1;
-    }
-    CUDA_TRY(cudaMemcpyAsync(b->d_qoff1, qo, sizeof(long long) * (n_ij + 1), cudaMemcpyHostToDevice, st));
-    long long t0[2] = {0, tot};
-    CUDA_TRY(cudaMemcpyAsync(b->d_task01, t0, sizeof(t0), cudaMemcpyHostToDevice, st));
-    JKSeg seg;
-    fill_seg(b, cp_ij, cp_kl, b->d_qoff1, n_ij, dm, n_dm, vj, vk, &seg);
     jk_launch_fn fn = g_tab64[class_index(b, cp_ij, cp_kl)];
     if (!fn) return set_err(JK_ERR_UNSUPPORTED, "no kernel for this class pair");
+    long long tot = 0;
+    int rc = class_pair_rows(b, bins_locs_ij, bins_locs_kl, nbins, n_ij, cp_ij == cp_kl, st, &tot);
+    if (rc) return rc;
+    JKSeg seg;
+    fill_seg(b, cp_ij, cp_kl, b->d_qoff1, n_ij, dm, n_dm, vj, vk, &seg);
     CUDA_TRY(fn(seg, b->d_task01, tot, b->nsm, st));
-    CUDA_TRY(cudaStreamSynchronize(st));
     return JK_OK;
 }
 
@@ -1016,37 +1062,14 @@ extern "C" int jk_fill_int2e(jk_basis_t* b, double* eri, int nao, const int* str
     const int n_ij = b->h_pair_locs[cp_ij + 1] - b->h_pair_locs[cp_ij];
     // kl bin kb pairs with ij in [bins_ij[0], bins_ij[nbins - kb]): row ij (in
     // bin sij) keeps kl < bins_kl[nbins - sij] (nr_fill_ao_ints.cu:519-545)
-    if ((size_t)n_ij + 1 > b->h_qoff1_cap) {
-        if (b->h_qoff1) cudaFreeHost(b->h_qoff1);
-        CUDA_TRY(cudaMallocHost(&b->h_qoff1, sizeof(long long) * (n_ij + 1)));
-        b->h_qoff1_cap = n_ij + 1;
-    }
-    CUDA_TRY(cudaStreamSynchronize(st));
-    long long* qo = b->h_qoff1;
-    qo[0] = 0;
-    int sij = 0;
     long long tot = 0;
-    for (int ij = 0; ij < n_ij; ij++) {
-        while (sij < nbins && ij >= bins_locs_ij[sij + 1]) sij++;
-        long long cnt = 0;
-        if (ij >= bins_locs_ij[0] && sij < nbins && bins_locs_kl[0] == 0) cnt = bins_locs_kl[nbins - sij];
-        tot += cnt;
-        qo[ij + 1] = tot;
-    }
-    if (n_ij + 1 > b->qoff1_cap) {
-        cudaFree(b->d_qoff1);
-        CUDA_TRY(cudaMalloc(&b->d_qoff1, sizeof(long long) * (n_ij + 1)));
-        b->qoff1_cap = n_ij + 1;
-    }
-    CUDA_TRY(cudaMemcpyAsync(b->d_qoff1, qo, sizeof(long long) * (n_ij + 1), cudaMemcpyHostToDevice, st));
-    long long t0[2] = {0, tot};
-    CUDA_TRY(cudaMemcpyAsync(b->d_task01, t0, sizeof(t0), cudaMemcpyHostToDevice, st));
+    int rc = class_pair_rows(b, bins_locs_ij, bins_locs_kl, nbins, n_ij, 0, st, &tot);
+    if (rc) return rc;
     JKSeg seg;
     fill_seg(b, cp_ij, cp_kl, b->d_qoff1, n_ij, nullptr, 0, nullptr, nullptr, &seg);
     long long s64[4];
     for (int a = 0; a < 4; a++) s64[a] = strides[a];
     CUDA_TRY(jk_launch_fill(seg, b->d_task01, tot, b->nsm, eri, s64, ao_offsets, st));
-    CUDA_TRY(cudaStreamSynchronize(st));
     return JK_OK;
 }
 

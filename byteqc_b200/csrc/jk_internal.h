@@ -134,8 +134,6 @@ struct jk_basis {
     long long* d_qoff1 = nullptr;
     long long* d_task01 = nullptr;
     long long qoff1_cap = 0;
-    long long* h_qoff1 = nullptr;  // pinned
-    size_t h_qoff1_cap = 0;
     JKFanout fan;  // side streams of the class launches
     double* d_pgeo = nullptr;  // pair geometry (JKSeg::pgeo)
     std::vector<int> h_pnp;    // primitive pairs above the exponent cutoff, per pair

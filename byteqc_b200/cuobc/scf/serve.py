@@ -257,6 +257,27 @@ class JKServer:
         return out
 
 
+def single_build_seconds(mol, cutoff=1e-13, fp32_cutoff=None):
+    """Seconds of one J/K build of ``mol`` alone on the GPU at the density
+    its request starts from (the core guess), after one untimed build: the
+    service time a request's iteration costs without batching, for sizing
+    an arrival rate.  (A diagonal or otherwise sparse density would let the
+    density screen drop most quartets and overstate the capacity.)"""
+    torch = hf._torch()
+    opt = hf._VHFOpt(mol).build(cutoff)
+    try:
+        st = _SCFState(_Request(-1, mol, 0., 1, None, None), opt, torch)
+        for _ in range(2):
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            hf.get_jk(mol, st.dm, vhfopt=opt, out='device',
+                      fp32_cutoff=fp32_cutoff)
+            torch.cuda.synchronize()
+        return time.perf_counter() - t
+    finally:
+        opt.clear()
+
+
 def poisson_serve(mols, rate_per_s, duration_s=None, seed=5, **server_kw):
     """Drive a JKServer with Poisson arrivals of ``mols`` (in order) at
     ``rate_per_s``; returns (server, wall seconds)."""

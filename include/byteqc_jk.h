@@ -82,7 +82,11 @@ int jk_basis_pairs(const jk_basis_t *basis, int *pair2shls, int *pair_locs, doub
  * GINTbuild_jk (cuobc/lib/gvhf/nr_jk_driver.cu:227-284): vj/vk are device
  * buffers (n_dm, nao, nao) accumulated (+=) with element (i, j) at
  * i + nao*j, either may be NULL; dm is the device density in the working
- * basis; bins are host arrays of nbins+1 offsets.
+ * basis; bins are host arrays of nbins+1 non-decreasing offsets, nbins <= 64.
+ * Asynchronous, as GINTbuild_jk: the bins are passed to the device by value
+ * (the host arrays may change once the call returns), the results are there
+ * once `stream` reaches them.  The calls of one basis handle share a
+ * row-prefix buffer: issue them on one stream (or order their streams).
  */
 int jk_build_class_pair(jk_basis_t *basis, double *vj, double *vk, const double *dm, int nao, int n_dm,
                         const int *bins_locs_ij, const int *bins_locs_kl, int nbins, int cp_ij, int cp_kl,
@@ -98,7 +102,8 @@ int jk_build_class_pair(jk_basis_t *basis, double *vj, double *vk, const double 
  * offsets o[4] (working-basis AO indices) host arrays.  Pairs on the
  * diagonal of a shell carry the basis's diagonal factor (1 with
  * diag_block_with_triu, else 1/2), as the reference's pair data do.  Every
- * class up to (hh|hh).
+ * class up to (ii|ii).  Asynchronous with the bin rules of
+ * jk_build_class_pair (nbins <= 64, one stream per basis handle).
  */
 int jk_fill_int2e(jk_basis_t *basis, double *eri, int nao, const int *strides, const int *ao_offsets,
                   const int *bins_locs_ij, const int *bins_locs_kl, int nbins, int cp_ij, int cp_kl, void *stream);
