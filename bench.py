@@ -294,11 +294,14 @@ def bench_serve(args, torch):
     mols = serve_workload(args.serve_requests, max_nbf=args.serve_max_nbf)
     nbf = [m.nao for m in mols]
     kw = dict(n_iter=args.serve_iters)
-    # warm-up: kernels, attributes, allocator
-    warm = JKServer(n_iter=2)
-    for m in mols[:2]:
-        warm.submit(m)
-    warm.run_until_empty()
+    # warm-up: one batched pass over every request in both precisions, so
+    # that the timed streams do not pay the first (lazy) load of a kernel,
+    # its attributes or the allocator's first blocks
+    for cut in (None, args.fp32_cutoff):
+        warm = JKServer(n_iter=1, fp32_cutoff=cut)
+        for m in mols:
+            warm.submit(m)
+        warm.run_until_empty()
     build_s = sum(single_build_seconds(m) for m in mols)
     cap_builds = len(mols) / build_s
     rate = 0.8 * cap_builds / args.serve_iters  # requests per second
