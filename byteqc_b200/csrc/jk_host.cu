@@ -1023,6 +1023,25 @@ static int class_pair_rows(jk_basis* b, const int* bins_ij, const int* bins_kl, 
     return JK_OK;
 }
 
+extern "C" int jk_class_pair_tasks(const int* bins_ij, const int* bins_kl, int nbins, int n_ij, int diag,
+                                   long long* qoff, long long* total) {
+    if (!bins_ij || !bins_kl || nbins <= 0 || nbins > JK_ROWBINS_MAX || n_ij < 0 || !total)
+        return set_err(JK_ERR_ARG, "jk_class_pair_tasks: invalid arguments");
+    JKRowBins rb;
+    rb.nbins = nbins;
+    rb.diag = diag ? 1 : 0;
+    for (int s = 0; s <= nbins; s++) {
+        rb.ij[s] = bins_ij[s];
+        rb.kl[s] = bins_kl[s];
+        if (s && (bins_ij[s] < bins_ij[s - 1] || bins_kl[s] < bins_kl[s - 1]))
+            return set_err(JK_ERR_ARG, "bins must not decrease");
+    }
+    if (qoff)
+        for (int r = 0; r <= n_ij; r++) qoff[r] = jk_rowbins_tasks(rb, r);
+    *total = jk_rowbins_tasks(rb, n_ij);
+    return JK_OK;
+}
+
 extern "C" int jk_build_class_pair(jk_basis_t* b, double* vj, double* vk, const double* dm, int nao, int n_dm,
                                    const int* bins_locs_ij, const int* bins_locs_kl, int nbins, int cp_ij,
                                    int cp_kl, void* stream) {

@@ -68,6 +68,9 @@ _SIGNATURES = {
     'jk_batch_create_ex': [ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong,
                            ctypes.c_void_p],
     'jk_batch_nsolo': [ctypes.c_void_p, ctypes.c_void_p],
+    'jk_class_pair_tasks': [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                            ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                            ctypes.c_void_p],
     'jk_batch_destroy': [ctypes.c_void_p],
     'jk_batch_build': [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                        ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,

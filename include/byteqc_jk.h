@@ -92,6 +92,15 @@ int jk_build_class_pair(jk_basis_t *basis, double *vj, double *vk, const double 
                         const int *bins_locs_ij, const int *bins_locs_kl, int nbins, int cp_ij, int cp_kl,
                         void *stream);
 
+/* Host only: the shell quartets a per-class-pair call computes for these
+ * bins (row ij of the class pair's n_ij shell pairs, in ij bin s, pairs with
+ * the kl pairs below bins_kl[nbins - s], as the reference's bin loop pairs
+ * kl bin b with ij bins below nbins - b, nr_jk_driver.cu:252-280; diag != 0:
+ * a diagonal class pair of jk_build_class_pair, kl <= ij).  qoff (may be
+ * NULL) receives the n_ij + 1 row prefixes, *total the count. */
+int jk_class_pair_tasks(const int *bins_ij, const int *bins_kl, int nbins, int n_ij, int diag, long long *qoff,
+                        long long *total);
+
 /*
  * ERI tensor of one class pair, same contract as GINTfill_int2e
  * (cuobc/lib/gint/nr_fill_ao_ints.cu:493-549): for every (ij, kl) the host

@@ -89,3 +89,52 @@ def test_shard_plan_balances_and_is_deterministic():
     bad = np.zeros(1, dtype=np.int32)
     assert lib.jk_shard_plan(None, 1, 2, bad.ctypes.data) == 3
     assert lib.jk_shard_plan(np.ones(1).ctypes.data, 1, 0, bad.ctypes.data) == 3
+
+
+def _ref_bin_loop_count(bins_ij, bins_kl, nbins, diag):
+    """The reference's bin loop (gvhf/nr_jk_driver.cu:252-280): kl bin b
+    pairs with the ij rows [bins_ij[0], bins_ij[nbins - b]); a diagonal
+    class pair keeps kl <= ij.  Returns the quartet count and the per-row
+    counts."""
+    rows = {}
+    n = 0
+    for b in range(nbins):
+        kl0, kl1 = bins_kl[b], bins_kl[b + 1]
+        for ij in range(bins_ij[0], bins_ij[nbins - b]):
+            c = sum(1 for kl in range(kl0, kl1) if not (diag and kl > ij))
+            rows[ij] = rows.get(ij, 0) + c
+            n += c
+    return n, rows
+
+
+def test_class_pair_tasks_follow_the_reference_bin_loop():
+    """The row prefix the per-class-pair entries build on the device (the
+    same code, run here on the host) counts exactly the quartets of the
+    reference's bin loop, on bins of seeded log-Schwarz values."""
+    from oracle import hf_oracle
+    lib = jklib.load_library()
+    rng = np.random.default_rng(3)
+    for it in range(60):
+        n_ij = int(rng.integers(1, 120))
+        diag = bool(it % 2)
+        n_kl = n_ij if diag else int(rng.integers(1, 120))
+        nbins = int(rng.integers(1, 16))
+        cutoff = 10.0 ** -rng.uniform(6, 14)
+        lq_ij = np.sort(rng.uniform(-30, 0, n_ij))[::-1]
+        lq_kl = np.sort(rng.uniform(-30, 0, n_kl))[::-1]
+        bij = hf_oracle.make_s_index_offsets(lq_ij, nbins, cutoff)
+        bkl = bij if diag else hf_oracle.make_s_index_offsets(lq_kl, nbins, cutoff)
+        qoff = np.zeros(n_ij + 1, dtype=np.int64)
+        tot = ctypes.c_longlong()
+        assert lib.jk_class_pair_tasks(bij.ctypes.data, bkl.ctypes.data, nbins, n_ij,
+                                       int(diag), qoff.ctypes.data, ctypes.byref(tot)) == 0
+        n, rows = _ref_bin_loop_count(bij, bkl, nbins, diag)
+        assert tot.value == n
+        per_row = np.diff(qoff)
+        for ij in range(n_ij):
+            assert per_row[ij] == rows.get(ij, 0), (it, ij)
+    # decreasing bins are refused
+    bad = np.array([0, 5, 3], dtype=np.int32)
+    tot = ctypes.c_longlong()
+    assert lib.jk_class_pair_tasks(bad.ctypes.data, bad.ctypes.data, 2, 5, 0, None,
+                                   ctypes.byref(tot)) == 3
