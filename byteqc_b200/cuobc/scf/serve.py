@@ -33,6 +33,18 @@ from byteqc_b200.cuobc.scf import hf
 from byteqc_b200.cuobc.scf.batch import JKBatch
 
 
+def _footprint(nbas, nao, nao0, npairs, nprim):
+    """Device bytes of an admitted request from its basis sizes: shell-pair
+    Schwarz matrix, pair lists and primitive-pair cache (basis handle),
+    density / J / K work buffers in the working basis and the back
+    transform, and the SCF state (S, H, orthogonaliser, density, DIIS
+    history) in the caller's basis."""
+    words = (nbas * nbas + 4 * npairs + 6 * nprim + 6 * npairs  # basis
+             + 6 * nao * nao + nao * nao0                       # work buffers
+             + 16 * nao0 * nao0)                                # SCF state
+    return 8 * words
+
+
 def footprint_bound_bytes(mol):
     """Upper bound of footprint_bytes(opt) from the basis alone (no device
     work, nothing allocated): every shell pair counted as kept by the
@@ -43,27 +55,18 @@ def footprint_bound_bytes(mol):
     ls = bas[:, 1]
     nps = bas[:, 2].astype(np.int64)
     nao = int(((ls + 1) * (ls + 2) // 2).sum())
-    nao0 = coeff.shape[1]
-    npairs = nbas * (nbas + 1) // 2
     nprim = int((nps.sum() ** 2 + (nps ** 2).sum()) // 2)
-    words = (nbas * nbas + 4 * npairs + 6 * nprim + 6 * npairs
-             + 6 * nao * nao + nao * nao0 + 16 * nao0 * nao0)
-    return 8 * words
+    return _footprint(nbas, nao, coeff.shape[1], nbas * (nbas + 1) // 2, nprim)
 
 
 def footprint_bytes(opt):
-    """Device bytes a request holds while admitted (basis, pair cache,
-    screening records, work buffers and SCF state), from the basis sizes."""
-    import ctypes
+    """Device bytes a request holds while admitted, from the sizes of its
+    basis handle (the shell pairs the Schwarz screen kept)."""
     from byteqc_b200.cuobc import lib as _lib
     info = np.zeros(7, dtype=np.int32)
     _lib.load_library().jk_basis_info(opt.handle, info.ctypes.data)
     nbas, nao, ngroups, ncp, npairs, nprim, ncq = (int(v) for v in info)
-    nao0 = opt.coeff.shape[1]
-    words = (nbas * nbas + 4 * npairs + 6 * nprim + 6 * npairs  # basis
-             + 6 * nao * nao + nao * nao0                       # work buffers
-             + 16 * nao0 * nao0)                                # SCF state
-    return 8 * words
+    return _footprint(nbas, nao, opt.coeff.shape[1], npairs, nprim)
 
 
 class _Request:

@@ -198,3 +198,32 @@ def test_bench_reference_arm_ranks():
     assert d['impl'] == 'reference' and d['value'] > 0
     assert d['cpu_baseline']['kind'] == 'port'
     assert d['e2e']['h2d_bytes_per_step'] == 0
+
+
+def test_serving_footprint_bound_covers_the_screened_basis():
+    """The server admits a request by a footprint bound computed before
+    anything is allocated: it is never below the footprint of the basis the
+    Schwarz screen keeps (pair lists from the oracle's restatement of
+    _VHFOpt.build), equals it when every shell pair is kept, and grows with
+    the molecule."""
+    from byteqc_b200.cuobc.scf.serve import _footprint, footprint_bound_bytes
+    from oracle import hf_oracle
+    prev = 0
+    for n in (3, 5, 8):
+        mol = Mole(atom=geom.random_walk_molecule(n, seed=60 + n),
+                   basis='standin-6-31g*').build()
+        opt = hf_oracle.VHFOpt(mol).build(1e-13)
+        pm = opt.mol
+        nbas = pm._bas.shape[0]
+        nps = pm._bas[:, 2].astype(np.int64)
+        i, j = opt.bas_pair2shls
+        nao = int(pm.ao_loc_nr(cart=True)[-1])
+        nao0 = opt.coeff.shape[1]
+        exact = _footprint(nbas, nao, nao0, i.size, int((nps[i] * nps[j]).sum()))
+        bound = footprint_bound_bytes(mol)
+        assert 0 < exact <= bound
+        all_pairs = nbas * (nbas + 1) // 2
+        all_prim = int((nps.sum() ** 2 + (nps ** 2).sum()) // 2)
+        assert _footprint(nbas, nao, nao0, all_pairs, all_prim) == bound
+        assert bound > prev
+        prev = bound
